@@ -1,0 +1,140 @@
+// Per-class host drivers: regroup the caller's lists on the device, then
+// launch the class's integral kernel, all on the caller's stream.
+#pragma once
+#include "engine.cuh"
+#include "jk_kernels.cuh"
+
+namespace vlxb {
+
+struct CoulombArgs {
+    double* mat_J;
+    const double* info[3];  // prim_info by angular momentum (s, p, d)
+    uint32_t count[3];      // prim_count by angular momentum
+    const double* cd_D;
+    const double* ab_Q;
+    const double* cd_Q;
+    const uint32_t* ab_first;
+    const uint32_t* ab_second;
+    const double* ab_pdata;
+    uint32_t n_ab;
+    const uint32_t* cd_first;
+    const uint32_t* cd_second;
+    const double* cd_pdata;
+    uint32_t n_cd;
+    double thr;
+};
+
+struct ExchangeArgs {
+    double* mat_K;
+    const uint32_t* pair_i;
+    const uint32_t* pair_k;
+    uint32_t n_ik;
+    const double* info[3];
+    const uint32_t* aoinds[3];
+    uint32_t count[3];
+    double maxD;
+    const double* D;
+    uint32_t naos;
+    const double *Q_ab, *Q_cd;
+    const uint32_t *Dinds_ab, *Dinds_cd;
+    const uint32_t *displs_ab, *displs_cd;
+    const uint32_t *counts_ab, *counts_cd;
+    const double *pdata_ab, *pdata_cd;
+    double omega;
+    double thr;
+};
+
+template <int LA, int LB, int LC, int LD>
+int run_coulomb(const CoulombArgs& a, cudaStream_t st)
+{
+    if (a.n_ab == 0 || a.n_cd == 0) return VLXB_OK;
+    if (!a.mat_J || !a.cd_D || !a.ab_Q || !a.cd_Q || !a.ab_first || !a.ab_second || !a.ab_pdata || !a.cd_first ||
+        !a.cd_second || !a.cd_pdata)
+        return VLXB_EINVAL;
+    const int L4[4] = {LA, LB, LC, LD};
+    for (int t = 0; t < 4; t++)
+        if (!a.info[L4[t]] || a.count[L4[t]] == 0) return VLXB_EINVAL;
+    if (!(a.thr >= 0.0)) return VLXB_EINVAL;
+    int rc = ensure_pool_configured();
+    if (rc) return rc;
+    const double* tab = boys_table_device();
+    if (!tab) return VLXB_ECUDA;
+    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    Arena ar(st);
+    PairGroups gb, gk;
+    rc = group_flat(ar, NA, NB, (int)a.count[LA], (int)a.count[LB], a.ab_first, a.ab_second, a.n_ab, a.info[LA],
+                    a.count[LA], a.info[LB], a.count[LB], gb);
+    if (rc) return rc;
+    rc = make_records(ar, NA * NB, gb, a.ab_Q, a.n_ab);
+    if (rc) return rc;
+    rc = group_flat(ar, NC, ND, (int)a.count[LC], (int)a.count[LD], a.cd_first, a.cd_second, a.n_cd, a.info[LC],
+                    a.count[LC], a.info[LD], a.count[LD], gk);
+    if (rc) return rc;
+    JKetData kd;
+    rc = jket_prepare<LC, LD>(ar, gk, a.cd_first, a.cd_second, a.cd_D, a.cd_Q, a.cd_pdata, kd);
+    if (rc) return rc;
+    JBraRecs bra{gb.rec_sp, gb.rec_q, gb.rec_mask, gb.n_rec, gb.geo, gb.entry, gb.sp_stride, a.ab_pdata};
+    JKetPairs ket{kd.geo, kd.tmax, kd.tmin, kd.Dpp, kd.Dm, kd.Qc, kd.Dc, kd.stride, kd.n};
+    int grid = launch_grid_limit();
+    if ((int64_t)grid > (int64_t)a.n_ab) grid = (int)a.n_ab;
+    coulomb_kernel<LA, LB, LC, LD><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    return VLXB_OK;
+}
+
+template <int LA, int LB, int LC, int LD>
+int run_exchange(const ExchangeArgs& a, cudaStream_t st)
+{
+    if (a.n_ik == 0) return VLXB_OK;
+    if (!a.mat_K || !a.pair_i || !a.pair_k || !a.D || !a.Q_ab || !a.Q_cd || !a.Dinds_ab || !a.Dinds_cd ||
+        !a.displs_ab || !a.displs_cd || !a.counts_ab || !a.counts_cd || !a.pdata_ab || !a.pdata_cd || a.naos == 0)
+        return VLXB_EINVAL;
+    const int L4[4] = {LA, LB, LC, LD};
+    for (int t = 0; t < 4; t++)
+        if (!a.info[L4[t]] || !a.aoinds[L4[t]] || a.count[L4[t]] == 0) return VLXB_EINVAL;
+    if (!(a.thr >= 0.0) || !(a.omega >= 0.0)) return VLXB_EINVAL;
+    int rc = ensure_pool_configured();
+    if (rc) return rc;
+    const double* tab = boys_table_device();
+    if (!tab) return VLXB_ECUDA;
+    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    Arena ar(st);
+    KOutData ko;
+    rc = kout_prepare(ar, NA, NC, (int)a.count[LA], (int)a.count[LC], a.pair_i, a.pair_k, a.n_ik, ko);
+    if (rc) return rc;
+    const int npa = (int)a.count[LA], npb = (int)a.count[LB], npc = (int)a.count[LC], npd = (int)a.count[LD];
+    PairGroups gab;
+    rc = group_csr(ar, NA, NB, npa, npb, a.displs_ab, a.counts_ab, a.Dinds_ab, (int64_t)npa * npb, a.info[LA],
+                   a.count[LA], a.info[LB], a.count[LB], gab);
+    if (rc) return rc;
+    rc = make_records(ar, NA * NB, gab, a.Q_ab, (int64_t)npa * npb * NA * NB);
+    if (rc) return rc;
+    rc = segment_records(ar, NA * NB, npa, npb, gab, a.pdata_ab);
+    if (rc) return rc;
+    PairGroups gcd;
+    const bool same = (LA == LC && LB == LD && a.Q_ab == a.Q_cd && a.Dinds_ab == a.Dinds_cd &&
+                       a.displs_ab == a.displs_cd && a.counts_ab == a.counts_cd && a.pdata_ab == a.pdata_cd);
+    if (same) {
+        gcd = gab;
+    } else {
+        rc = group_csr(ar, NC, ND, npc, npd, a.displs_cd, a.counts_cd, a.Dinds_cd, (int64_t)npc * npd, a.info[LC],
+                       a.count[LC], a.info[LD], a.count[LD], gcd);
+        if (rc) return rc;
+        rc = make_records(ar, NC * ND, gcd, a.Q_cd, (int64_t)npc * npd * NC * ND);
+        if (rc) return rc;
+        rc = segment_records(ar, NC * ND, npc, npd, gcd, a.pdata_cd);
+        if (rc) return rc;
+    }
+    KOutBlocks out{ko.ish, ko.ksh, ko.idx, ko.stride, ko.n};
+    KPartnerRecs rab{gab.rec_sp, gab.rec_q, gab.rec_mask, gab.seg, gab.geo, gab.S, gab.sp_j, gab.sp_stride};
+    KPartnerRecs rcd{gcd.rec_sp, gcd.rec_q, gcd.rec_mask, gcd.seg, gcd.geo, gcd.S, gcd.sp_j, gcd.sp_stride};
+    int grid = launch_grid_limit();
+    if ((int64_t)grid > (int64_t)a.n_ik) grid = (int)a.n_ik;
+    exchange_kernel<LA, LB, LC, LD><<<grid, K_THREADS, 0, st>>>(out, rab, rcd, a.aoinds[LB], a.count[LB],
+                                                                a.aoinds[LD], a.count[LD], a.D, a.naos, a.maxD,
+                                                                a.omega, a.thr, a.mat_K, tab);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    return VLXB_OK;
+}
+
+}  // namespace vlxb

@@ -1,0 +1,122 @@
+// Host-side engine pieces shared by all class translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <vector>
+
+#include "common.cuh"
+
+namespace vlxb {
+
+// Status codes returned through the C ABI.
+enum Status : int {
+    VLXB_OK = 0,
+    VLXB_EINVAL = 1,   // invalid argument (null pointer, bad count or class)
+    VLXB_ECUDA = 2,    // a CUDA runtime call failed
+    VLXB_ENOMEM = 3,   // device allocation failed
+};
+
+#define VLXB_CHECK_CUDA(call)                              \
+    do {                                                   \
+        cudaError_t _e = (call);                           \
+        if (_e != cudaSuccess) return (_e == cudaErrorMemoryAllocation) ? VLXB_ENOMEM : VLXB_ECUDA; \
+    } while (0)
+
+// Stream-ordered scratch arena: every buffer is taken from the device's
+// default memory pool with cudaMallocAsync on the call's stream and handed
+// back with cudaFreeAsync when the arena goes out of scope, so scratch is
+// reused across calls without synchronisation.
+class Arena {
+  public:
+    explicit Arena(cudaStream_t s) : stream_(s) {}
+    ~Arena()
+    {
+        for (void* p : ptrs_) cudaFreeAsync(p, stream_);
+    }
+    Arena(const Arena&) = delete;
+    Arena& operator=(const Arena&) = delete;
+
+    template <typename T>
+    T* alloc(int64_t n)
+    {
+        if (failed_) return nullptr;
+        void* p = nullptr;
+        size_t bytes = (size_t)(n > 0 ? n : 1) * sizeof(T);
+        if (cudaMallocAsync(&p, bytes, stream_) != cudaSuccess) {
+            failed_ = true;
+            cudaGetLastError();
+            return nullptr;
+        }
+        ptrs_.push_back(p);
+        return (T*)p;
+    }
+    bool failed() const { return failed_; }
+    cudaStream_t stream() const { return stream_; }
+
+  private:
+    cudaStream_t stream_;
+    std::vector<void*> ptrs_;
+    bool failed_ = false;
+};
+
+// Per-device FP64 Boys table (BOYS_NGRID x BOYS_NCOL), built on first use.
+// Returns nullptr on failure.  The first call on a device synchronises it
+// (table upload); call vlxb_init() before any stream capture.
+const double* boys_table_device();
+
+// Make the device's default memory pool keep freed scratch (release
+// threshold = max) so per-call scratch costs no new cudaMalloc after warm-up.
+int ensure_pool_configured();
+
+// ---------------------------------------------------------------- prep API
+struct PairGroups {
+    int* spidx = nullptr;      // [npa * npb] exclusive scan of the occupancy table
+    int* n_sp = nullptr;       // device count of shell pairs
+    int64_t sp_stride = 0;     // allocation bound of shell-pair arrays
+    int32_t* sp_i = nullptr;   // [sp_stride]
+    int32_t* sp_j = nullptr;   // [sp_stride]
+    int32_t* entry = nullptr;  // [NXY][sp_stride] caller list position or -1
+    double* geo = nullptr;     // [GEO_N][sp_stride]
+    int* n_rec = nullptr;      // device count of records
+    int64_t rec_stride = 0;
+    int32_t* rec_sp = nullptr;
+    double* rec_q = nullptr;
+    uint64_t* rec_mask = nullptr;
+    int* seg = nullptr;        // [npa + 1] (segmented records only)
+    double* S = nullptr;       // [NXY][sp_stride] (partner records only)
+};
+
+// Group a flat list of prim-cart pairs (first[e], second[e]) by shell pair.
+int group_flat(Arena& ar, int na, int nb, int npa, int npb, const uint32_t* first, const uint32_t* second,
+               int64_t n, const double* info_a, uint32_t cnt_a, const double* info_b, uint32_t cnt_b,
+               PairGroups& g);
+// Group a CSR partner list (per prim-cart i: displs, counts, Dinds) by shell pair.
+int group_csr(Arena& ar, int na, int nb, int npa, int npb, const uint32_t* displs, const uint32_t* counts,
+              const uint32_t* Dinds, int64_t n_entries_bound, const double* info_a, uint32_t cnt_a,
+              const double* info_b, uint32_t cnt_b, PairGroups& g);
+// Split shell pairs into uniform-Q records (Q indexed by caller list position).
+int make_records(Arena& ar, int nxy, PairGroups& g, const double* Q, int64_t n_entries);
+// Sort records by descending q inside segments of the first primitive shell,
+// and fill per-shell-pair S from the caller's pair data.
+int segment_records(Arena& ar, int nxy, int npa, int npb, PairGroups& g, const double* pdata);
+
+struct JKetData {
+    double *geo, *tmax, *tmin, *Dpp, *Dm, *Qc, *Dc;
+    int64_t stride;
+    int* n;
+};
+template <int LC, int LD>
+int jket_prepare(Arena& ar, const PairGroups& g, const uint32_t* first, const uint32_t* second,
+                 const double* D, const double* Q, const double* pdata, JKetData& out);
+
+struct KOutData {
+    int32_t *ish, *ksh, *idx;
+    int64_t stride;
+    int* n;
+};
+int kout_prepare(Arena& ar, int na, int nc, int npa, int npc, const uint32_t* pi, const uint32_t* pk, int64_t n,
+                 KOutData& out);
+
+int launch_grid_limit();
+
+}  // namespace vlxb

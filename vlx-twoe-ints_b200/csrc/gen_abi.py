@@ -1,0 +1,231 @@
+"""Writes the C-ABI boundary of the engine.
+
+Outputs:
+  include/vlxb.h                  public C header (committed)
+  csrc/generated/abi.cu           the extern "C" entry points
+  csrc/generated/cls_<abcd>_j.cu  one translation unit per Coulomb class
+  csrc/generated/cls_<abcd>_k.cu  one translation unit per exchange class
+
+Entry-point names and argument lists mirror the kernels the reference
+generator emits, so a caller that binds those kernels binds these instead:
+  computeCoulombFock<ABCD>   gen_coulomb.py:74-93, classes gen_coulomb.py:47-56
+  computeExchangeFock<ABCD>  gen_exchange.py:75-115 (identical in
+                             new_exchange_code/exchangefockwriter.py:55-104),
+                             classes new_exchange_code/gen_eri_exchange.py:39-56
+Each entry point takes one extra trailing argument, the CUDA stream (void*,
+NULL = default stream), and returns a status code instead of void.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+ANG = "spd"
+LV = {"s": 0, "p": 1, "d": 2}
+
+
+def j_classes():
+    pairs = [a + b for i, a in enumerate(ANG) for b in ANG[i:]]
+    return [ab + cd for ab in pairs for cd in pairs]
+
+
+def k_classes():
+    out = []
+    for i, a in enumerate(ANG):
+        for c in ANG[i:]:
+            for b in ANG:
+                for d in ANG:
+                    out.append(a + b + c + d)
+    return out
+
+
+def j_params(cls):
+    a, b, c, d = cls
+    p = ["double* mat_J"]
+    for x in ANG:
+        if x in cls:
+            p += [f"const double* {x}_prim_info", f"uint32_t {x}_prim_count"]
+    p += [f"const double* {c}{d}_mat_D", f"const double* {a}{b}_mat_Q_local", f"const double* {c}{d}_mat_Q",
+          f"const uint32_t* {a}{b}_first_inds_local", f"const uint32_t* {a}{b}_second_inds_local",
+          f"const double* {a}{b}_pair_data_local", f"uint32_t {a}{b}_prim_pair_count_local",
+          f"const uint32_t* {c}{d}_first_inds", f"const uint32_t* {c}{d}_second_inds",
+          f"const double* {c}{d}_pair_data", f"uint32_t {c}{d}_prim_pair_count",
+          "const double* boys_func_table", "const double* boys_func_ft", "double eri_threshold",
+          "void* stream"]
+    return p
+
+
+def k_params(cls):
+    a, b, c, d = cls
+    same = (c + d) == (a + b)
+    p = ["double* mat_K", f"const uint32_t* pair_inds_i_for_K_{a}{c}", f"const uint32_t* pair_inds_k_for_K_{a}{c}",
+         f"uint32_t pair_inds_count_for_K_{a}{c}"]
+    for x in ANG:
+        if x in cls:
+            p += [f"const double* {x}_prim_info", f"const uint32_t* {x}_prim_aoinds", f"uint32_t {x}_prim_count"]
+    p += [f"double {b}{d}_max_D", "const double* mat_D_full_AO", "uint32_t naos"]
+    for typ, nm in (("const double*", "Q_K"), ("const uint32_t*", "D_inds_K"), ("const uint32_t*", "pair_displs_K"),
+                    ("const uint32_t*", "pair_counts_K"), ("const double*", "pair_data_K")):
+        p.append(f"{typ} {nm}_{a}{b}")
+        if not same:
+            p.append(f"{typ} {nm}_{c}{d}")
+    p += ["const double* boys_func_table", "const double* boys_func_ft", "double omega", "double eri_threshold",
+          "void* stream"]
+    return p
+
+
+def pname(p):
+    return p.split()[-1]
+
+
+def header():
+    L = ["/*",
+         " * vlxb.h -- C ABI of the B200 (sm_100a) two-electron J/K engine.",
+         " *",
+         " * Drop-in for the CUDA/HIP kernels that VeloxChem's vlx-twoe-ints generator",
+         " * emits.  Every computeCoulombFock<ABCD> / computeExchangeFock<ABCD> kernel of",
+         " * the reference has one entry point here, vlxb_computeCoulombFock<ABCD> /",
+         " * vlxb_computeExchangeFock<ABCD>, with the same arguments in the same order and",
+         " * the same meaning, plus a trailing CUDA stream (void*, NULL = default stream).",
+         " *",
+         " * Conventions (as for the reference kernels):",
+         " *  - every pointer is caller-owned DEVICE memory; mat_J / mat_K are accumulated",
+         " *    with += (zero them first for a fresh build);",
+         " *  - prim-cart index i of type x is primitive shell i / ncart(x), Cartesian",
+         " *    component i % ncart(x) (p: x,y,z; d: xx,xy,xz,yy,yz,zz);",
+         " *  - prim_info is [5][prim_count] (row 0 exponent, rows 2..4 centre);",
+         " *    prim_aoinds is [ncart][prim_count] (AO index of each component);",
+         " *  - screening keeps a term iff |Q_ij Q_kl D_kl| > eri_threshold (J) or",
+         " *    |Q_ij Q_kl max_D| > eri_threshold (K).  This is the set the reference's",
+         " *    per-thread `break` selects when its ket/partner lists are sorted by",
+         " *    descending bound; here no ordering of the input lists is required.",
+         " *  - boys_func_table / boys_func_ft are accepted for signature compatibility",
+         " *    and ignored: the engine carries its own FP64 Boys table.",
+         " *  - work is enqueued on `stream`; calls do not synchronise the host.",
+         " *    Scratch comes from the device's default memory pool (cudaMallocAsync).",
+         " *  - return value: VLXB_OK or an error code (never traps).",
+         " */",
+         "#ifndef VLXB_H", "#define VLXB_H", "", "#include <stdint.h>", "",
+         "#ifdef __cplusplus", 'extern "C" {', "#endif", "",
+         "#define VLXB_OK 0", "#define VLXB_EINVAL 1", "#define VLXB_ECUDA 2", "#define VLXB_ENOMEM 3", "",
+         "/* Select `device`, configure its memory pool and upload the Boys table.",
+         "   Call once per device before any stream capture.  No reference",
+         "   counterpart (the reference's caller owns its Boys table). */",
+         "int vlxb_init(int device);", "",
+         "/* Human-readable text for a status code.  No reference counterpart. */",
+         "const char* vlxb_status_string(int status);", "",
+         "/* ABI version (major * 10000 + minor * 100 + patch).  No reference counterpart. */",
+         "int vlxb_version(void);", ""]
+    L.append("/* ---- Coulomb: replace computeCoulombFock<ABCD> of gen_coulomb.py:74-93 ---- */")
+    for cls in j_classes():
+        L.append(f"/* replaces computeCoulombFock{cls.upper()} (gen_coulomb.py:74-93; class list gen_coulomb.py:47-56) */")
+        L.append(f"int vlxb_computeCoulombFock{cls.upper()}(" + ", ".join(j_params(cls)) + ");")
+    L.append("")
+    L.append("/* ---- Exchange: replace computeExchangeFock<ABCD> of gen_exchange.py:75-115 ---- */")
+    for cls in k_classes():
+        L.append(f"/* replaces computeExchangeFock{cls.upper()} (gen_exchange.py:75-115; "
+                 "class list new_exchange_code/gen_eri_exchange.py:39-56) */")
+        L.append(f"int vlxb_computeExchangeFock{cls.upper()}(" + ", ".join(k_params(cls)) + ");")
+    L += ["", "#ifdef __cplusplus", "}", "#endif", "", "#endif /* VLXB_H */", ""]
+    return "\n".join(L)
+
+
+def abi_cu():
+    L = ["// Generated by gen_abi.py -- do not edit.",
+         '#include "../classes.cuh"',
+         '#include "../../../include/vlxb.h"', "",
+         "namespace vlxb {"]
+    for cls in j_classes():
+        la, lb, lc, ld = (LV[x] for x in cls)
+        L.append(f"int coulomb_{cls}(const CoulombArgs&, cudaStream_t);")
+    for cls in k_classes():
+        L.append(f"int exchange_{cls}(const ExchangeArgs&, cudaStream_t);")
+    L += ["}  // namespace vlxb", "", 'extern "C" {', ""]
+    for cls in j_classes():
+        a, b, c, d = cls
+        ps = j_params(cls)
+        L.append(f"int vlxb_computeCoulombFock{cls.upper()}(" + ", ".join(ps) + ")")
+        L.append("{")
+        L.append("    (void)boys_func_table; (void)boys_func_ft;")
+        L.append("    vlxb::CoulombArgs A{};")
+        L.append("    A.mat_J = mat_J;")
+        for x in ANG:
+            if x in cls:
+                L.append(f"    A.info[{LV[x]}] = {x}_prim_info; A.count[{LV[x]}] = {x}_prim_count;")
+        L += [f"    A.cd_D = {c}{d}_mat_D; A.ab_Q = {a}{b}_mat_Q_local; A.cd_Q = {c}{d}_mat_Q;",
+              f"    A.ab_first = {a}{b}_first_inds_local; A.ab_second = {a}{b}_second_inds_local;",
+              f"    A.ab_pdata = {a}{b}_pair_data_local; A.n_ab = {a}{b}_prim_pair_count_local;",
+              f"    A.cd_first = {c}{d}_first_inds; A.cd_second = {c}{d}_second_inds;",
+              f"    A.cd_pdata = {c}{d}_pair_data; A.n_cd = {c}{d}_prim_pair_count;",
+              "    A.thr = eri_threshold;",
+              f"    return vlxb::coulomb_{cls}(A, (cudaStream_t)stream);", "}", ""]
+    for cls in k_classes():
+        a, b, c, d = cls
+        same = (c + d) == (a + b)
+        ps = k_params(cls)
+        L.append(f"int vlxb_computeExchangeFock{cls.upper()}(" + ", ".join(ps) + ")")
+        L.append("{")
+        L.append("    (void)boys_func_table; (void)boys_func_ft;")
+        L.append("    vlxb::ExchangeArgs A{};")
+        L.append(f"    A.mat_K = mat_K; A.pair_i = pair_inds_i_for_K_{a}{c}; A.pair_k = pair_inds_k_for_K_{a}{c};")
+        L.append(f"    A.n_ik = pair_inds_count_for_K_{a}{c};")
+        for x in ANG:
+            if x in cls:
+                L.append(f"    A.info[{LV[x]}] = {x}_prim_info; A.aoinds[{LV[x]}] = {x}_prim_aoinds; "
+                         f"A.count[{LV[x]}] = {x}_prim_count;")
+        L.append(f"    A.maxD = {b}{d}_max_D; A.D = mat_D_full_AO; A.naos = naos;")
+        cd = f"{a}{b}" if same else f"{c}{d}"
+        L.append(f"    A.Q_ab = Q_K_{a}{b}; A.Q_cd = Q_K_{cd};")
+        L.append(f"    A.Dinds_ab = D_inds_K_{a}{b}; A.Dinds_cd = D_inds_K_{cd};")
+        L.append(f"    A.displs_ab = pair_displs_K_{a}{b}; A.displs_cd = pair_displs_K_{cd};")
+        L.append(f"    A.counts_ab = pair_counts_K_{a}{b}; A.counts_cd = pair_counts_K_{cd};")
+        L.append(f"    A.pdata_ab = pair_data_K_{a}{b}; A.pdata_cd = pair_data_K_{cd};")
+        L.append("    A.omega = omega; A.thr = eri_threshold;")
+        L.append(f"    return vlxb::exchange_{cls}(A, (cudaStream_t)stream);")
+        L += ["}", ""]
+    L += ["}  // extern \"C\"", ""]
+    return "\n".join(L)
+
+
+def class_tu(cls, kind):
+    la, lb, lc, ld = (LV[x] for x in cls)
+    L = ["// Generated by gen_abi.py -- do not edit.",
+         '#include "../common.cuh"',
+         f'#include "q_{cls}.cuh"',
+         '#include "hrr_pairs.cuh"',
+         '#include "../classes.cuh"', "",
+         "namespace vlxb {"]
+    if kind == "j":
+        L.append(f"int coulomb_{cls}(const CoulombArgs& a, cudaStream_t s) "
+                 f"{{ return run_coulomb<{la}, {lb}, {lc}, {ld}>(a, s); }}")
+    else:
+        L.append(f"int exchange_{cls}(const ExchangeArgs& a, cudaStream_t s) "
+                 f"{{ return run_exchange<{la}, {lb}, {lc}, {ld}>(a, s); }}")
+    L += ["}  // namespace vlxb", ""]
+    return "\n".join(L)
+
+
+def write_if_changed(path, text):
+    if os.path.exists(path):
+        with open(path) as fh:
+            if fh.read() == text:
+                return
+    with open(path, "w") as fh:
+        fh.write(text)
+
+
+def main(pkg_root, repo_root):
+    gen = os.path.join(pkg_root, "csrc", "generated")
+    os.makedirs(gen, exist_ok=True)
+    write_if_changed(os.path.join(repo_root, "include", "vlxb.h"), header())
+    write_if_changed(os.path.join(gen, "abi.cu"), abi_cu())
+    for cls in j_classes():
+        write_if_changed(os.path.join(gen, f"cls_{cls}_j.cu"), class_tu(cls, "j"))
+    for cls in k_classes():
+        write_if_changed(os.path.join(gen, f"cls_{cls}_k.cu"), class_tu(cls, "k"))
+
+
+if __name__ == "__main__":
+    here = os.path.dirname(os.path.abspath(__file__))
+    pkg = os.path.dirname(here)
+    main(pkg, os.path.dirname(pkg))

@@ -1,0 +1,344 @@
+// Host orchestration of the device-side list regrouping (see prep.cuh), the
+// per-device Boys table and memory-pool set-up.
+#include <cub/cub.cuh>
+#include <math.h>
+#include <mutex>
+
+#include "common.cuh"
+#include "engine.cuh"
+#include "generated/hrr_pairs.cuh"
+#include "prep.cuh"
+
+namespace vlxb {
+
+// ------------------------------------------------------------ Boys table
+// F_m(T_k) for T_k = k*BOYS_H, m < BOYS_NCOL, from the convergent series
+// F_m(T) = e^{-T} sum_{i>=0} (2T)^i / ((2m+1)(2m+3)...(2m+2i+1)) in long
+// double, with downward recursion for the lower orders.
+static void build_boys_host(std::vector<double>& tab)
+{
+    tab.assign((size_t)BOYS_NGRID * BOYS_NCOL, 0.0);
+    const int M = BOYS_NCOL - 1;
+    for (int k = 0; k < BOYS_NGRID; k++) {
+        const long double T = (long double)k * (long double)BOYS_H;
+        long double F[BOYS_NCOL];
+        long double term = 1.0L / (2.0L * M + 1.0L), sum = term;
+        for (int i = 1; i < 4000; i++) {
+            term *= 2.0L * T / (2.0L * M + 2.0L * i + 1.0L);
+            sum += term;
+            if (i > T && term < 1e-25L * sum) break;
+        }
+        const long double ex = expl(-T);
+        F[M] = ex * sum;
+        for (int m = M - 1; m >= 0; m--) F[m] = (2.0L * T * F[m + 1] + ex) / (2.0L * m + 1.0L);
+        for (int m = 0; m < BOYS_NCOL; m++) tab[(size_t)k * BOYS_NCOL + m] = (double)F[m];
+    }
+}
+
+static std::mutex g_mu;
+static const double* g_boys_dev[64] = {nullptr};
+static bool g_pool_done[64] = {false};
+
+const double* boys_table_device()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_boys_dev[dev]) return g_boys_dev[dev];
+    static std::vector<double> host;
+    if (host.empty()) build_boys_host(host);
+    double* d = nullptr;
+    if (cudaMalloc(&d, host.size() * sizeof(double)) != cudaSuccess) return nullptr;
+    if (cudaMemcpy(d, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(d);
+        return nullptr;
+    }
+    g_boys_dev[dev] = d;
+    return d;
+}
+
+int ensure_pool_configured()
+{
+    int dev = 0;
+    VLXB_CHECK_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return VLXB_EINVAL;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_pool_done[dev]) return VLXB_OK;
+    cudaMemPool_t pool;
+    VLXB_CHECK_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t thr = UINT64_MAX;
+    VLXB_CHECK_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    g_pool_done[dev] = true;
+    return VLXB_OK;
+}
+
+int launch_grid_limit()
+{
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms * 16;
+}
+
+// ------------------------------------------------------------ helpers
+static int scan_int(Arena& ar, const int* in, int* out, int64_t n)
+{
+    size_t bytes = 0;
+    VLXB_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, (int)n, ar.stream()));
+    void* tmp = ar.alloc<char>((int64_t)bytes);
+    if (!tmp) return VLXB_ENOMEM;
+    VLXB_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, (int)n, ar.stream()));
+    return VLXB_OK;
+}
+
+static int finish_grouping(Arena& ar, int64_t ntab, int* table, PairGroups& g)
+{
+    cudaStream_t st = ar.stream();
+    g.spidx = ar.alloc<int>(ntab);
+    g.n_sp = ar.alloc<int>(1);
+    if (!g.spidx || !g.n_sp) return VLXB_ENOMEM;
+    int rc = scan_int(ar, table, g.spidx, ntab);
+    if (rc) return rc;
+    k_scan_total<<<1, 1, 0, st>>>(g.spidx, table, ntab, g.n_sp);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    return VLXB_OK;
+}
+
+static int alloc_sp(Arena& ar, int nxy, PairGroups& g)
+{
+    g.sp_i = ar.alloc<int32_t>(g.sp_stride);
+    g.sp_j = ar.alloc<int32_t>(g.sp_stride);
+    g.entry = ar.alloc<int32_t>(g.sp_stride * nxy);
+    g.geo = ar.alloc<double>(g.sp_stride * GEO_N);
+    if (ar.failed()) return VLXB_ENOMEM;
+    VLXB_CHECK_CUDA(cudaMemsetAsync(g.entry, 0xFF, sizeof(int32_t) * g.sp_stride * nxy, ar.stream()));
+    return VLXB_OK;
+}
+
+int group_flat(Arena& ar, int na, int nb, int npa, int npb, const uint32_t* first, const uint32_t* second,
+               int64_t n, const double* info_a, uint32_t cnt_a, const double* info_b, uint32_t cnt_b,
+               PairGroups& g)
+{
+    cudaStream_t st = ar.stream();
+    const int64_t ntab = (int64_t)npa * npb;
+    int* table = ar.alloc<int>(ntab);
+    if (!table) return VLXB_ENOMEM;
+    VLXB_CHECK_CUDA(cudaMemsetAsync(table, 0, sizeof(int) * ntab, st));
+    k_mark_pairs<<<prep_blocks(n), PREP_THREADS, 0, st>>>(first, second, n, na, nb, npb, table);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    int rc = finish_grouping(ar, ntab, table, g);
+    if (rc) return rc;
+    g.sp_stride = n < ntab ? n : ntab;
+    rc = alloc_sp(ar, na * nb, g);
+    if (rc) return rc;
+    k_fill_pairs<<<prep_blocks(n), PREP_THREADS, 0, st>>>(first, second, n, na, nb, npb, g.spidx, g.entry, g.sp_i,
+                                                          g.sp_j, g.sp_stride);
+    k_pair_geo<<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.sp_i, g.sp_j, info_a, cnt_a, info_b,
+                                                                   cnt_b, g.geo, g.sp_stride);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    return VLXB_OK;
+}
+
+int group_csr(Arena& ar, int na, int nb, int npa, int npb, const uint32_t* displs, const uint32_t* counts,
+              const uint32_t* Dinds, int64_t n_entries_bound, const double* info_a, uint32_t cnt_a,
+              const double* info_b, uint32_t cnt_b, PairGroups& g)
+{
+    cudaStream_t st = ar.stream();
+    const int64_t ntab = (int64_t)npa * npb;
+    const int n_first = npa * na;
+    int* table = ar.alloc<int>(ntab);
+    if (!table) return VLXB_ENOMEM;
+    VLXB_CHECK_CUDA(cudaMemsetAsync(table, 0, sizeof(int) * ntab, st));
+    k_mark_csr<<<prep_blocks(n_first), PREP_THREADS, 0, st>>>(displs, counts, Dinds, n_first, na, nb, npb, table);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    int rc = finish_grouping(ar, ntab, table, g);
+    if (rc) return rc;
+    g.sp_stride = n_entries_bound < ntab ? n_entries_bound : ntab;
+    rc = alloc_sp(ar, na * nb, g);
+    if (rc) return rc;
+    k_fill_csr<<<prep_blocks(n_first), PREP_THREADS, 0, st>>>(displs, counts, Dinds, n_first, na, nb, npb, g.spidx,
+                                                              g.entry, g.sp_i, g.sp_j, g.sp_stride);
+    k_pair_geo<<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.sp_i, g.sp_j, info_a, cnt_a, info_b,
+                                                                   cnt_b, g.geo, g.sp_stride);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    return VLXB_OK;
+}
+
+template <int NXY>
+static void launch_rec_count(const PairGroups& g, const double* Q, int* nrec, cudaStream_t st)
+{
+    k_rec_count<NXY><<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, g.sp_stride, Q, nrec);
+}
+template <int NXY>
+static void launch_rec_fill(const PairGroups& g, const double* Q, const int* recoff, cudaStream_t st)
+{
+    k_rec_fill<NXY><<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, g.sp_stride, Q, recoff,
+                                                                       g.rec_sp, g.rec_q, g.rec_mask);
+}
+template <int NXY>
+static void launch_sp_S(const PairGroups& g, const double* pdata, cudaStream_t st)
+{
+    k_sp_S<NXY><<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, g.sp_stride, pdata, g.S);
+}
+
+#define VLXB_NXY_DISPATCH(nxy, FN, ...)            \
+    switch (nxy) {                                 \
+        case 1: FN<1>(__VA_ARGS__); break;         \
+        case 3: FN<3>(__VA_ARGS__); break;         \
+        case 6: FN<6>(__VA_ARGS__); break;         \
+        case 9: FN<9>(__VA_ARGS__); break;         \
+        case 18: FN<18>(__VA_ARGS__); break;       \
+        case 36: FN<36>(__VA_ARGS__); break;       \
+        default: return VLXB_EINVAL;               \
+    }
+
+int make_records(Arena& ar, int nxy, PairGroups& g, const double* Q, int64_t n_entries)
+{
+    cudaStream_t st = ar.stream();
+    int64_t bound = g.sp_stride * nxy;
+    g.rec_stride = bound < n_entries ? bound : n_entries;
+    if (g.rec_stride < g.sp_stride) g.rec_stride = g.sp_stride;
+    int* nrec = ar.alloc<int>(g.sp_stride + 1);
+    int* recoff = ar.alloc<int>(g.sp_stride + 1);
+    g.n_rec = ar.alloc<int>(1);
+    g.rec_sp = ar.alloc<int32_t>(g.rec_stride);
+    g.rec_q = ar.alloc<double>(g.rec_stride);
+    g.rec_mask = ar.alloc<uint64_t>(g.rec_stride);
+    if (ar.failed()) return VLXB_ENOMEM;
+    VLXB_CHECK_CUDA(cudaMemsetAsync(nrec, 0, sizeof(int) * (g.sp_stride + 1), st));
+    VLXB_NXY_DISPATCH(nxy, launch_rec_count, g, Q, nrec, st);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    int rc = scan_int(ar, nrec, recoff, g.sp_stride + 1);
+    if (rc) return rc;
+    k_scan_total<<<1, 1, 0, st>>>(recoff, nrec, g.sp_stride + 1, g.n_rec);
+    VLXB_NXY_DISPATCH(nxy, launch_rec_fill, g, Q, recoff, st);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    // keep recoff for segment offsets
+    g.seg = recoff;  // temporarily: record offsets per shell pair
+    return VLXB_OK;
+}
+
+int segment_records(Arena& ar, int nxy, int npa, int npb, PairGroups& g, const double* pdata)
+{
+    cudaStream_t st = ar.stream();
+    const int* recoff = g.seg;
+    int* seg = ar.alloc<int>(npa + 1);
+    double* q_sorted = ar.alloc<double>(g.rec_stride);
+    int* perm_in = ar.alloc<int>(g.rec_stride);
+    int* perm = ar.alloc<int>(g.rec_stride);
+    int32_t* sp_sorted = ar.alloc<int32_t>(g.rec_stride);
+    uint64_t* mask_sorted = ar.alloc<uint64_t>(g.rec_stride);
+    g.S = ar.alloc<double>(g.sp_stride * nxy);
+    if (ar.failed()) return VLXB_ENOMEM;
+    k_rec_segments<<<prep_blocks(npa + 1), PREP_THREADS, 0, st>>>(g.spidx, recoff, npa, npb, g.n_rec, seg);
+    k_iota<<<prep_blocks(g.rec_stride), PREP_THREADS, 0, st>>>(perm_in, g.rec_stride);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    size_t bytes = 0;
+    VLXB_CHECK_CUDA(cub::DeviceSegmentedRadixSort::SortPairsDescending(
+        nullptr, bytes, g.rec_q, q_sorted, perm_in, perm, (int)g.rec_stride, npa, seg, seg + 1, 0, 64, st));
+    void* tmp = ar.alloc<char>((int64_t)bytes);
+    if (!tmp) return VLXB_ENOMEM;
+    VLXB_CHECK_CUDA(cub::DeviceSegmentedRadixSort::SortPairsDescending(
+        tmp, bytes, g.rec_q, q_sorted, perm_in, perm, (int)g.rec_stride, npa, seg, seg + 1, 0, 64, st));
+    k_gather_recs<<<prep_blocks(g.rec_stride), PREP_THREADS, 0, st>>>(g.n_rec, perm, g.rec_sp, g.rec_mask,
+                                                                       sp_sorted, mask_sorted);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    g.rec_q = q_sorted;
+    g.rec_sp = sp_sorted;
+    g.rec_mask = mask_sorted;
+    g.seg = seg;
+    VLXB_NXY_DISPATCH(nxy, launch_sp_S, g, pdata, st);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    return VLXB_OK;
+}
+
+template <int LC, int LD>
+int jket_prepare(Arena& ar, const PairGroups& g, const uint32_t* first, const uint32_t* second,
+                 const double* D, const double* Q, const double* pdata, JKetData& out)
+{
+    constexpr int NCD = ncart(LC) * ncart(LD), NF = nrange(LC, LD);
+    cudaStream_t st = ar.stream();
+    const int64_t S = g.sp_stride;
+    double* keys = ar.alloc<double>(S);
+    double* keys_sorted = ar.alloc<double>(S);
+    int* perm_in = ar.alloc<int>(S);
+    int* perm = ar.alloc<int>(S);
+    double* tmin_u = ar.alloc<double>(S);
+    double* Dpp_u = ar.alloc<double>(S * NF);
+    double* Dm_u = ar.alloc<double>(S * NCD);
+    double* Qc_u = ar.alloc<double>(S * NCD);
+    double* Dc_u = ar.alloc<double>(S * NCD);
+    out.geo = ar.alloc<double>(S * GEO_N);
+    out.tmin = ar.alloc<double>(S);
+    out.tmax = ar.alloc<double>(S);
+    out.Dpp = ar.alloc<double>(S * NF);
+    out.Dm = ar.alloc<double>(S * NCD);
+    out.Qc = ar.alloc<double>(S * NCD);
+    out.Dc = ar.alloc<double>(S * NCD);
+    if (ar.failed()) return VLXB_ENOMEM;
+    out.stride = S;
+    out.n = g.n_sp;
+    k_jket_fill<LC, LD><<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, S, first, second, D, Q, pdata,
+                                                                 g.geo, keys, tmin_u, Dpp_u, Dm_u, Qc_u, Dc_u, S);
+    k_iota<<<prep_blocks(S), PREP_THREADS, 0, st>>>(perm_in, S);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    size_t bytes = 0;
+    VLXB_CHECK_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, keys, keys_sorted, perm_in, perm,
+                                                              (int)S, 0, 64, st));
+    void* tmp = ar.alloc<char>((int64_t)bytes);
+    if (!tmp) return VLXB_ENOMEM;
+    VLXB_CHECK_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp, bytes, keys, keys_sorted, perm_in, perm, (int)S,
+                                                              0, 64, st));
+    k_jket_gather<LC, LD><<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, perm, S, g.geo, keys_sorted, tmin_u,
+                                                                   Dpp_u, Dm_u, Qc_u, Dc_u, out.geo, out.tmax,
+                                                                   out.tmin, out.Dpp, out.Dm, out.Qc, out.Dc);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    return VLXB_OK;
+}
+
+template int jket_prepare<0, 0>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
+                                const double*, const double*, JKetData&);
+template int jket_prepare<0, 1>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
+                                const double*, const double*, JKetData&);
+template int jket_prepare<0, 2>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
+                                const double*, const double*, JKetData&);
+template int jket_prepare<1, 1>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
+                                const double*, const double*, JKetData&);
+template int jket_prepare<1, 2>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
+                                const double*, const double*, JKetData&);
+template int jket_prepare<2, 2>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
+                                const double*, const double*, JKetData&);
+
+template <int NAC>
+static void launch_kout(const uint32_t* pi, const uint32_t* pk, int64_t n, int na, int nc, int npc, const int* spidx,
+                        KOutData& out, cudaStream_t st)
+{
+    k_kout_fill<NAC><<<prep_blocks(n), PREP_THREADS, 0, st>>>(pi, pk, n, na, nc, npc, spidx, out.idx, out.ish,
+                                                              out.ksh, out.stride);
+}
+
+int kout_prepare(Arena& ar, int na, int nc, int npa, int npc, const uint32_t* pi, const uint32_t* pk, int64_t n,
+                 KOutData& out)
+{
+    cudaStream_t st = ar.stream();
+    const int64_t ntab = (int64_t)npa * npc;
+    int* table = ar.alloc<int>(ntab);
+    if (!table) return VLXB_ENOMEM;
+    VLXB_CHECK_CUDA(cudaMemsetAsync(table, 0, sizeof(int) * ntab, st));
+    k_mark_pairs<<<prep_blocks(n), PREP_THREADS, 0, st>>>(pi, pk, n, na, nc, npc, table);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    PairGroups g;
+    int rc = finish_grouping(ar, ntab, table, g);
+    if (rc) return rc;
+    out.stride = n < ntab ? n : ntab;
+    out.n = g.n_sp;
+    out.ish = ar.alloc<int32_t>(out.stride);
+    out.ksh = ar.alloc<int32_t>(out.stride);
+    out.idx = ar.alloc<int32_t>(out.stride * na * nc);
+    if (ar.failed()) return VLXB_ENOMEM;
+    VLXB_CHECK_CUDA(cudaMemsetAsync(out.idx, 0xFF, sizeof(int32_t) * out.stride * na * nc, st));
+    VLXB_NXY_DISPATCH(na * nc, launch_kout, pi, pk, n, na, nc, npc, g.spidx, out, st);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    return VLXB_OK;
+}
+
+}  // namespace vlxb

@@ -1,0 +1,301 @@
+// Device-side regrouping of the reference's primitive-Cartesian pair lists
+// into primitive-SHELL-pair records (the unit of the integral kernels).
+//
+// Reference list formats (gen_coulomb.py:80-90, gen_exchange.py:78-110):
+//   prim-cart index i of type x -> primitive shell i / ncart(x), component
+//   i % ncart(x); prim_info[5][count] (row 0 exponent, rows 2-4 xyz);
+//   J lists: first/second prim-cart indices, pair_data S_ij_00, Q, D per pair;
+//   K lists: CSR per prim-cart i (displs, counts) of partners D_inds with Q
+//   and pair_data; prim_aoinds[ncart][count] maps (primitive, component) to
+//   the Cartesian AO index.
+//
+// Grouping uses a dense table over (shell_i, shell_j) and an exclusive scan,
+// so record order is deterministic (shell-major) and no atomics are needed.
+// Every count that sizes a later launch stays on the device (grid-stride
+// kernels read it), so a whole ABI call issues no host synchronisation.
+#pragma once
+#include "common.cuh"
+
+namespace vlxb {
+
+constexpr int PREP_THREADS = 256;
+
+__host__ __forceinline__ int prep_blocks(int64_t n)
+{
+    int64_t b = (n + PREP_THREADS - 1) / PREP_THREADS;
+    if (b < 1) b = 1;
+    if (b > 148 * 32) b = 148 * 32;
+    return (int)b;
+}
+
+__global__ void k_iota(int* __restrict__ p, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = (int)i;
+}
+
+// ------------------------------------------------------------ flat lists
+
+__global__ void k_mark_pairs(const uint32_t* __restrict__ first, const uint32_t* __restrict__ second,
+                             int64_t n, int na, int nb, int npb, int* __restrict__ table)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t key = (int64_t)(first[e] / na) * npb + second[e] / nb;
+        table[key] = 1;
+    }
+}
+
+__global__ void k_fill_pairs(const uint32_t* __restrict__ first, const uint32_t* __restrict__ second,
+                             int64_t n, int na, int nb, int npb, const int* __restrict__ spidx,
+                             int32_t* __restrict__ entry, int32_t* __restrict__ sp_i, int32_t* __restrict__ sp_j,
+                             int64_t stride)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t i = first[e], j = second[e];
+        const int64_t key = (int64_t)(i / na) * npb + j / nb;
+        const int s = spidx[key];
+        const int comp = (int)(i % na) * nb + (int)(j % nb);
+        entry[comp * stride + s] = (int32_t)e;
+        sp_i[s] = (int32_t)(i / na);
+        sp_j[s] = (int32_t)(j / nb);
+    }
+}
+
+// ------------------------------------------------------------ CSR lists
+
+__global__ void k_mark_csr(const uint32_t* __restrict__ displs, const uint32_t* __restrict__ counts,
+                           const uint32_t* __restrict__ Dinds, int n_first, int na, int nb, int npb,
+                           int* __restrict__ table)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_first; i += gridDim.x * blockDim.x) {
+        const uint32_t d0 = displs[i], c = counts[i];
+        for (uint32_t t = 0; t < c; t++) {
+            const uint32_t j = Dinds[d0 + t];
+            table[(int64_t)(i / na) * npb + j / nb] = 1;
+        }
+    }
+}
+
+__global__ void k_fill_csr(const uint32_t* __restrict__ displs, const uint32_t* __restrict__ counts,
+                           const uint32_t* __restrict__ Dinds, int n_first, int na, int nb, int npb,
+                           const int* __restrict__ spidx, int32_t* __restrict__ entry,
+                           int32_t* __restrict__ sp_i, int32_t* __restrict__ sp_j, int64_t stride)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_first; i += gridDim.x * blockDim.x) {
+        const uint32_t d0 = displs[i], c = counts[i];
+        for (uint32_t t = 0; t < c; t++) {
+            const uint32_t j = Dinds[d0 + t];
+            const int s = spidx[(int64_t)(i / na) * npb + j / nb];
+            const int comp = (i % na) * nb + (int)(j % nb);
+            entry[comp * stride + s] = (int32_t)(d0 + t);
+            sp_i[s] = i / na;
+            sp_j[s] = (int32_t)(j / nb);
+        }
+    }
+}
+
+// n_out[0] = scan[n-1] + flag[n-1]  (exclusive scan total)
+__global__ void k_scan_total(const int* __restrict__ scan, const int* __restrict__ flag, int64_t n, int* __restrict__ out)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[0] = (n > 0) ? scan[n - 1] + flag[n - 1] : 0;
+}
+
+// Pair geometry (see PairGeo): z, 0.5/z, P, P - A, A - B.
+__global__ void k_pair_geo(const int* __restrict__ n_sp, const int32_t* __restrict__ sp_i,
+                           const int32_t* __restrict__ sp_j, const double* __restrict__ info_a, uint32_t cnt_a,
+                           const double* __restrict__ info_b, uint32_t cnt_b, double* __restrict__ geo,
+                           int64_t stride)
+{
+    const int n = *n_sp;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const int i = sp_i[s], j = sp_j[s];
+        const double ai = info_a[i], aj = info_b[j];
+        const double A[3] = {info_a[i + 2 * (int64_t)cnt_a], info_a[i + 3 * (int64_t)cnt_a], info_a[i + 4 * (int64_t)cnt_a]};
+        const double B[3] = {info_b[j + 2 * (int64_t)cnt_b], info_b[j + 3 * (int64_t)cnt_b], info_b[j + 4 * (int64_t)cnt_b]};
+        const double z = ai + aj, iz = 1.0 / z;
+        geo[G_Z * stride + s] = z;
+        geo[G_I2Z * stride + s] = 0.5 * iz;
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+            const double P = (ai * A[x] + aj * B[x]) * iz;
+            geo[(G_PX + x) * stride + s] = P;
+            geo[(G_AX + x) * stride + s] = P - A[x];
+            geo[(G_RX + x) * stride + s] = A[x] - B[x];
+        }
+    }
+}
+
+// ------------------------------------------------------------ records
+// A record is a subset of one shell pair's components that share one Schwarz
+// value q (the caller may give every component its own Q).  Record =
+// (shell pair, q, component bitmask).  Records of a shell pair follow the
+// first appearance of each distinct q in component order.
+
+template <int NXY>
+__global__ void k_rec_count(const int* __restrict__ n_sp, const int32_t* __restrict__ entry, int64_t stride,
+                            const double* __restrict__ Q, int* __restrict__ nrec)
+{
+    const int n = *n_sp;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        double qs[NXY];
+        int nd = 0;
+        for (int c = 0; c < NXY; c++) {
+            const int32_t e = entry[c * stride + s];
+            if (e < 0) continue;
+            const double v = Q[e];
+            bool seen = false;
+            for (int t = 0; t < nd; t++) seen |= (qs[t] == v);
+            if (!seen) qs[nd++] = v;
+        }
+        nrec[s] = nd;
+    }
+}
+
+template <int NXY>
+__global__ void k_rec_fill(const int* __restrict__ n_sp, const int32_t* __restrict__ entry, int64_t stride,
+                           const double* __restrict__ Q, const int* __restrict__ recoff,
+                           int32_t* __restrict__ rec_sp, double* __restrict__ rec_q, uint64_t* __restrict__ rec_mask)
+{
+    const int n = *n_sp;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        double qs[NXY];
+        uint64_t ms[NXY];
+        int nd = 0;
+        for (int c = 0; c < NXY; c++) {
+            const int32_t e = entry[c * stride + s];
+            if (e < 0) continue;
+            const double v = Q[e];
+            int t = 0;
+            for (; t < nd; t++) if (qs[t] == v) break;
+            if (t == nd) { qs[nd] = v; ms[nd] = 0; nd++; }
+            ms[t] |= (1ull << c);
+        }
+        const int r0 = recoff[s];
+        for (int t = 0; t < nd; t++) {
+            rec_sp[r0 + t] = s;
+            rec_q[r0 + t] = qs[t];
+            rec_mask[r0 + t] = ms[t];
+        }
+    }
+}
+
+// S per shell pair and component (0 where the caller has no entry).
+template <int NXY>
+__global__ void k_sp_S(const int* __restrict__ n_sp, const int32_t* __restrict__ entry, int64_t stride,
+                       const double* __restrict__ pdata, double* __restrict__ S)
+{
+    const int n = *n_sp;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x)
+        for (int c = 0; c < NXY; c++) {
+            const int32_t e = entry[c * stride + s];
+            S[c * stride + s] = (e >= 0) ? pdata[e] : 0.0;
+        }
+}
+
+// Segment offsets of records by first shell: seg[i] = recoff[spidx[i * npb]],
+// seg[np_first] = total records.
+__global__ void k_rec_segments(const int* __restrict__ spidx, const int* __restrict__ recoff, int np_first, int npb,
+                               const int* __restrict__ n_rec, int* __restrict__ seg)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= np_first; i += gridDim.x * blockDim.x)
+        seg[i] = (i < np_first) ? recoff[spidx[(int64_t)i * npb]] : *n_rec;
+}
+
+__global__ void k_gather_recs(const int* __restrict__ n_rec, const int* __restrict__ perm,
+                              const int32_t* __restrict__ sp_in, const uint64_t* __restrict__ mask_in,
+                              int32_t* __restrict__ sp_out, uint64_t* __restrict__ mask_out)
+{
+    const int n = *n_rec;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const int p = perm[r];
+        sp_out[r] = sp_in[p];
+        mask_out[r] = mask_in[p];
+    }
+}
+
+// ------------------------------------------------------------ J ket data
+// Per ket shell pair: |Q D| bounds, per-component Q and D (for the exact
+// screen), Dm = w * D * S with the k<->l weight of gen_coulomb.py:276-281,
+// and Dpp = transposed ket HRR of Dm.
+template <int LC, int LD>
+__global__ void k_jket_fill(const int* __restrict__ n_sp, const int32_t* __restrict__ entry, int64_t stride,
+                            const uint32_t* __restrict__ first, const uint32_t* __restrict__ second,
+                            const double* __restrict__ Dlist, const double* __restrict__ Qlist,
+                            const double* __restrict__ pdata, const double* __restrict__ geo,
+                            double* __restrict__ tmax_key, double* __restrict__ tmin,
+                            double* __restrict__ Dpp, double* __restrict__ Dm, double* __restrict__ Qc,
+                            double* __restrict__ Dc, int64_t key_len)
+{
+    constexpr int NCD = ncart(LC) * ncart(LD), NF = nrange(LC, LD);
+    const int n = *n_sp;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < key_len; s += (int64_t)gridDim.x * blockDim.x) {
+        if (s >= n) { tmax_key[s] = -1.0; continue; }
+        double dm[NCD];
+        double tx = 0.0, tn = 1.0e300;
+        for (int c = 0; c < NCD; c++) {
+            const int32_t e = entry[c * stride + s];
+            double q = 0.0, d = 0.0, m = 0.0;
+            if (e >= 0) {
+                q = Qlist[e];
+                d = Dlist[e];
+                const double w = (LC != LD) ? 2.0 : ((first[e] != second[e]) ? 2.0 : 1.0);
+                m = w * d * pdata[e];
+                const double t = fabs(q * d);
+                tx = fmax(tx, t);
+                tn = fmin(tn, t);
+            }
+            dm[c] = m;
+            Qc[c * stride + s] = q;
+            Dc[c * stride + s] = d;
+            Dm[c * stride + s] = m;
+        }
+        tmax_key[s] = tx;
+        tmin[s] = tn;
+        double dpp[NF];
+        hrr_ket_adjoint<LC, LD>(geo[G_RX * stride + s], geo[G_RY * stride + s], geo[G_RZ * stride + s], dm, dpp);
+        for (int f = 0; f < NF; f++) Dpp[f * stride + s] = dpp[f];
+    }
+}
+
+// Gather ket arrays into the sorted order given by perm.
+template <int LC, int LD>
+__global__ void k_jket_gather(const int* __restrict__ n_sp, const int* __restrict__ perm, int64_t stride,
+                              const double* __restrict__ geo_in, const double* __restrict__ tmax_in,
+                              const double* __restrict__ tmin_in, const double* __restrict__ Dpp_in,
+                              const double* __restrict__ Dm_in, const double* __restrict__ Qc_in,
+                              const double* __restrict__ Dc_in, double* __restrict__ geo, double* __restrict__ tmax,
+                              double* __restrict__ tmin, double* __restrict__ Dpp, double* __restrict__ Dm,
+                              double* __restrict__ Qc, double* __restrict__ Dc)
+{
+    constexpr int NCD = ncart(LC) * ncart(LD), NF = nrange(LC, LD);
+    const int n = *n_sp;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const int p = perm[r];
+        for (int g = 0; g < GEO_N; g++) geo[g * stride + r] = geo_in[g * stride + p];
+        tmax[r] = tmax_in[r];  // keys are already sorted
+        tmin[r] = tmin_in[p];
+        for (int f = 0; f < NF; f++) Dpp[f * stride + r] = Dpp_in[f * stride + p];
+        for (int c = 0; c < NCD; c++) {
+            Dm[c * stride + r] = Dm_in[c * stride + p];
+            Qc[c * stride + r] = Qc_in[c * stride + p];
+            Dc[c * stride + r] = Dc_in[c * stride + p];
+        }
+    }
+}
+
+// ------------------------------------------------------------ K outputs
+template <int NAC>
+__global__ void k_kout_fill(const uint32_t* __restrict__ pi, const uint32_t* __restrict__ pk, int64_t n,
+                            int na, int nc, int npc, const int* __restrict__ spidx, int32_t* __restrict__ idx,
+                            int32_t* __restrict__ ish, int32_t* __restrict__ ksh, int64_t stride)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t i = pi[e], k = pk[e];
+        const int s = spidx[(int64_t)(i / na) * npc + k / nc];
+        idx[((i % na) * nc + (k % nc)) * stride + s] = (int32_t)e;
+        ish[s] = i / na;
+        ksh[s] = k / nc;
+    }
+}
+
+}  // namespace vlxb
