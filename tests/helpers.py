@@ -1,0 +1,79 @@
+"""Shared test helpers: oracle-backed Schwarz values and oracle J/K over
+reference-format lists (the oracle is the checker; see oracle/__init__.py)."""
+from __future__ import annotations
+
+import numpy as np
+
+from oracle import oracle
+from vlxb.lists import ANG, LV, ReferenceLists
+
+
+def oracle_schwarz_fn(la, lb, pd, P, Q):
+    out = np.zeros(len(P))
+    ia, ib = pd.info[la], pd.info[lb]
+    for t, (p, q) in enumerate(zip(P, Q)):
+        A, B = ia[2:5, p], ib[2:5, q]
+        I = oracle.eri_shell_quartet(la, lb, la, lb, ia[0, p], A, ib[0, q], B, ia[0, p], A, ib[0, q], B)
+        n = I.shape[0] * I.shape[1]
+        out[t] = np.sqrt(np.abs(np.diag(I.reshape(n, n))).max())
+    return out
+
+
+def oracle_J(rl: ReferenceLists, cls: str, rows=None):
+    a, b, c, d = cls
+    jab, jcd = rl.jlists[a + b], rl.jlists[c + d]
+    return oracle.coulomb_fock(LV[a], LV[b], LV[c], LV[d], rl.pd.info, rl.pd.count, jcd.D, jab.Q, jcd.Q,
+                               jab.first, jab.second, jab.pdata, jcd.first, jcd.second, jcd.pdata,
+                               rl.threshold, rows=rows)
+
+
+def oracle_K(rl: ReferenceLists, cls: str, omega=0.0, rows=None):
+    a, b, c, d = cls
+    kq = rl.kpairs[a + c]
+    p1, p2 = rl.kpartners[a + b], rl.kpartners[c + d]
+    return oracle.exchange_fock(LV[a], LV[b], LV[c], LV[d], kq.pair_i, kq.pair_k, rl.pd.info, rl.pd.aoinds,
+                                rl.pd.count, rl.maxD[b + d], rl.D_AO, p1.Q, p2.Q, p1.Dinds, p2.Dinds, p1.displs,
+                                p2.displs, p1.counts, p2.counts, p1.pdata, p2.pdata, omega, rl.threshold,
+                                rows=rows)
+
+
+def oracle_jk_all(rl: ReferenceLists, omega=0.0):
+    from vlxb.lists import j_classes, k_classes
+
+    matJ = {k: np.zeros(len(v.first)) for k, v in rl.jlists.items()}
+    matK = {k: np.zeros(len(v.pair_i)) for k, v in rl.kpairs.items()}
+    for cls in j_classes():
+        if cls[:2] in rl.jlists and cls[2:] in rl.jlists:
+            matJ[cls[:2]] += oracle_J(rl, cls)
+    for cls in k_classes():
+        if cls[0] + cls[2] in rl.kpairs and cls[:2] in rl.kpartners and cls[2:] in rl.kpartners:
+            matK[cls[0] + cls[2]] += oracle_K(rl, cls, omega)
+    return matJ, matK
+
+
+def ao_eri_tensor(mol):
+    """Full contracted Cartesian AO ERI tensor from the oracle (tiny systems only)."""
+    from vlxb.basis import NCART
+
+    n = mol.naos
+    G = np.zeros((n, n, n, n))
+    sh = mol.shells
+    for A in sh:
+        for B in sh:
+            for C in sh:
+                for D in sh:
+                    blk = np.zeros((NCART[A.l], NCART[B.l], NCART[C.l], NCART[D.l]))
+                    for ea, ca in zip(A.exps, A.coefs):
+                        for eb, cb in zip(B.exps, B.coefs):
+                            for ec, cc in zip(C.exps, C.coefs):
+                                for ed, cd in zip(D.exps, D.coefs):
+                                    RA, RB = mol.coords[A.atom], mol.coords[B.atom]
+                                    RC, RD = mol.coords[C.atom], mol.coords[D.atom]
+                                    p, q = ea + eb, ec + ed
+                                    Sab = ca * cb * (np.pi / p) ** 1.5 * np.exp(-ea * eb / p * np.sum((RA - RB) ** 2))
+                                    Scd = cc * cd * (np.pi / q) ** 1.5 * np.exp(-ec * ed / q * np.sum((RC - RD) ** 2))
+                                    blk += Sab * Scd * oracle.eri_shell_quartet(A.l, B.l, C.l, D.l, ea, RA, eb, RB,
+                                                                                ec, RC, ed, RD)
+                    G[A.ao0:A.ao0 + NCART[A.l], B.ao0:B.ao0 + NCART[B.l], C.ao0:C.ao0 + NCART[C.l],
+                      D.ao0:D.ao0 + NCART[D.l]] = blk
+    return G

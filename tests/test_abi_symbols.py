@@ -1,0 +1,52 @@
+"""The C-ABI library loads and exports every function include/vlxb.h declares
+(no compute calls: these run without a GPU)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HDR = os.path.join(ROOT, "include", "vlxb.h")
+LIBP = os.path.join(ROOT, "vlx-twoe-ints_b200", "vlxb", "libvlxb.so")
+
+
+def declared():
+    txt = open(HDR).read()
+    return re.findall(r"^(?:int|const char\*)\s+(vlxb_\w+)\(", txt, flags=re.M)
+
+
+def test_header_lists_all_reference_classes():
+    names = declared()
+    j = [n for n in names if n.startswith("vlxb_computeCoulombFock")]
+    k = [n for n in names if n.startswith("vlxb_computeExchangeFock")]
+    assert len(j) == 36 and len(k) == 54
+    assert "vlxb_computeCoulombFockDDDD" in j and "vlxb_computeExchangeFockSDPD" in k and "vlxb_computeExchangeFockPDSD" not in k
+
+
+def test_library_exports_every_declared_symbol():
+    if not os.path.exists(LIBP):
+        pytest.fail("libvlxb.so is not built (python -m vlxb.build)")
+    lib = ctypes.CDLL(LIBP)
+    missing = [n for n in declared() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_status_strings_and_version():
+    lib = ctypes.CDLL(LIBP)
+    lib.vlxb_status_string.restype = ctypes.c_char_p
+    assert lib.vlxb_status_string(0) == b"ok"
+    assert lib.vlxb_status_string(1) == b"invalid argument"
+    assert lib.vlxb_version() >= 100
+
+
+def test_python_binding_matches_header():
+    from vlxb._lib import ABI
+
+    hdr = open(HDR).read()
+    for cls in ABI.j_classes():
+        sig = f"int vlxb_computeCoulombFock{cls.upper()}(" + ", ".join(ABI.j_params(cls)) + ");"
+        assert sig in hdr
+    for cls in ABI.k_classes():
+        sig = f"int vlxb_computeExchangeFock{cls.upper()}(" + ", ".join(ABI.k_params(cls)) + ");"
+        assert sig in hdr

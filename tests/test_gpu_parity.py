@@ -1,0 +1,225 @@
+"""GPU parity: every J and K entry point, called through the C ABI, against
+the reference-generated golden fixture and against the CPU oracle.
+
+Tolerance (FP64 mode): max |GPU - expected| <= 1e-10 * max |expected| + 1e-14
+per class and list, the bar of 1e-10 stated for the FP64 build.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+import helpers
+import tiny_fixture as tf
+from vlxb import basis, fock, lists
+from vlxb._lib import lib
+from vlxb.fock import DeviceLists
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-10
+
+
+def close(got, exp):
+    scale = float(np.abs(exp).max()) if exp.size else 0.0
+    return float(np.abs(got - exp).max()) <= RTOL * scale + 1e-14 if exp.size else True
+
+
+def fixture_lists(z, thr):
+    dev = torch.device("cuda")
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    U = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint32).view(np.int32)).to(dev)
+    info, aoinds, count = tf.prim_tables(z)
+    dl = DeviceLists(device=dev, naos=int(z["naos"][0]), threshold=thr, count=count)
+    dl.D_AO = T(z["D_AO"])
+    for l in range(3):
+        dl.info[l] = T(info[l])
+        dl.aoinds[l] = U(aoinds[l])
+    for ab in ("ss", "sp", "sd", "pp", "pd", "dd"):
+        dl.j[ab] = {"first": U(z[f"J_{ab}_first"]), "second": U(z[f"J_{ab}_second"]),
+                    "pdata": T(z[f"J_{ab}_pdata"]), "Q": T(z[f"J_{ab}_Q"]), "D": T(z[f"J_{ab}_D"])}
+    for a in "spd":
+        for b in "spd":
+            dl.kpart[a + b] = {"displs": U(z[f"K_{a}{b}_displs"]), "counts": U(z[f"K_{a}{b}_counts"]),
+                               "Dinds": U(z[f"K_{a}{b}_Dinds"]), "Q": T(z[f"K_{a}{b}_Q"]),
+                               "pdata": T(z[f"K_{a}{b}_pdata"])}
+    for i, a in enumerate("spd"):
+        for c in "spd"[i:]:
+            dl.kpair[a + c] = {"i": U(z[f"K_{a}{c}_pair_i"]), "k": U(z[f"K_{a}{c}_pair_k"])}
+    for cls in tf.k_classes():
+        dl.maxD[cls[1] + cls[3]] = float(z[f"K_{cls}_maxD"][0])
+    return dl
+
+
+@pytest.fixture(scope="module")
+def golden():
+    lib().init(0)
+    return tf.load()
+
+
+@pytest.mark.parametrize("tag", ["t12", "t3"])
+def test_golden_all_coulomb_classes(golden, tag):
+    z = golden
+    dl = fixture_lists(z, tf.THRESHOLDS[tag])
+    s = torch.cuda.current_stream().cuda_stream
+    bad = []
+    for cls in tf.j_classes():
+        out = torch.zeros(dl.j[cls[:2]]["first"].numel(), dtype=torch.float64, device="cuda")
+        lib().coulomb(cls, fock.coulomb_args(dl, cls, out, s))
+        got = out.cpu().numpy()
+        if not close(got, z[f"J_{cls}_{tag}"]):
+            bad.append((cls, float(np.abs(got - z[f"J_{cls}_{tag}"]).max())))
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("variant", tf.K_VARIANTS, ids=[v[0] for v in tf.K_VARIANTS])
+def test_golden_all_exchange_classes(golden, variant):
+    z = golden
+    tag, thr, omega, nrow = variant
+    dl = fixture_lists(z, thr)
+    s = torch.cuda.current_stream().cuda_stream
+    bad = []
+    for cls in tf.k_classes():
+        ac = cls[0] + cls[2]
+        out = torch.zeros(dl.kpair[ac]["i"].numel(), dtype=torch.float64, device="cuda")
+        lib().exchange(cls, fock.exchange_args(dl, cls, out, s, omega))
+        got = out.cpu().numpy()
+        exp = z[f"K_{cls}_{tag}"]
+        if nrow is not None:
+            got = got[:len(exp)]
+        if not close(got, exp):
+            bad.append((cls, float(np.abs(got - exp).max())))
+    assert not bad, bad
+
+
+def small_system(recipe, natoms, side, degree=2, alpha0=0.3, ratio=2.5, nocc=4, thr=1e-12, seed=11):
+    wl = basis.config_custom(natoms, side, recipe, degree, alpha0, ratio, nocc, thr, seed)
+    rl = lists.build_lists(wl.mol, wl.D, thr, fock.gpu_schwarz_fn())
+    return wl, rl
+
+
+def test_gpu_schwarz_matches_oracle():
+    lib().init(0)
+    wl = basis.config_custom(2, 3.0, {0: 1, 1: 1, 2: 1}, 2, 0.4, 2.3, 3, 1e-12, 5)
+    pd = lists.prim_data(wl.mol)
+    g = fock.gpu_schwarz_fn()
+    for la in range(3):
+        for lb in range(la, 3):
+            sp_g = lists.all_shell_pairs(pd, la, lb, g)
+            sp_o = lists.all_shell_pairs(pd, la, lb, helpers.oracle_schwarz_fn)
+            assert np.allclose(sp_g.q, sp_o.q, rtol=1e-12, atol=1e-300)
+
+
+def test_spd_molecule_full_vs_oracle():
+    """Two atoms with s, p and d shells: every J/K class vs the oracle, AO J/K
+    and the energy Tr[D(J - K/2)]."""
+    lib().init(0)
+    wl, rl = small_system({0: 1, 1: 1, 2: 1}, 2, 3.0)
+    dl = fock.to_device(rl)
+    matJ, matK = fock.build_jk(dl)
+    torch.cuda.synchronize()
+    oJ, oK = helpers.oracle_jk_all(rl)
+    for k in oJ:
+        assert close(matJ[k].cpu().numpy(), oJ[k]), k
+    for k in oK:
+        assert close(matK[k].cpu().numpy(), oK[k]), k
+    J = lists.contract_J(rl, {k: v.cpu().numpy() for k, v in matJ.items()})
+    K = lists.contract_K(rl, {k: v.cpu().numpy() for k, v in matK.items()})
+    Jo, Ko = lists.contract_J(rl, oJ), lists.contract_K(rl, oK)
+    assert np.abs(J - Jo).max() <= 1e-10 * np.abs(Jo).max()
+    assert np.abs(K - Ko).max() <= 1e-10 * np.abs(Ko).max()
+    assert abs(lists.energy(wl.D, J, K) - lists.energy(wl.D, Jo, Ko)) < 1e-10
+
+
+def test_range_separated_exchange_vs_oracle():
+    lib().init(0)
+    wl, rl = small_system({0: 1, 1: 1, 2: 1}, 2, 3.0, seed=13)
+    dl = fock.to_device(rl)
+    _, matK = fock.build_jk(dl, omega=0.33, do_j=False)
+    torch.cuda.synchronize()
+    _, oK = helpers.oracle_jk_all(rl, omega=0.33)
+    for k in oK:
+        assert close(matK[k].cpu().numpy(), oK[k]), k
+
+
+def test_small_sp_workload_sampled_rows():
+    """The 5-atom 3s+2p workload (45 Cartesian AOs): 48 random rows of every
+    class against the oracle."""
+    lib().init(0)
+    wl = basis.config_small(0)
+    rl = lists.build_lists(wl.mol, wl.D, wl.threshold, fock.gpu_schwarz_fn())
+    dl = fock.to_device(rl)
+    matJ, matK = fock.build_jk(dl)
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(0)
+    for ab in rl.jlists:
+        n = len(rl.jlists[ab].first)
+        rows = np.sort(rng.choice(n, size=min(48, n), replace=False))
+        exp = np.zeros(n)
+        for cd in rl.jlists:
+            if lists.LV[cd[0]] <= lists.LV[cd[1]]:
+                exp += helpers.oracle_J(rl, ab + cd, rows=rows)
+        assert close(matJ[ab].cpu().numpy()[rows], exp[rows]), ab
+    for ac in rl.kpairs:
+        n = len(rl.kpairs[ac].pair_i)
+        rows = np.sort(rng.choice(n, size=min(48, n), replace=False))
+        exp = np.zeros(n)
+        for b in "sp":
+            for d in "sp":
+                exp += helpers.oracle_K(rl, ac[0] + b + ac[1] + d, rows=rows)
+        assert close(matK[ac].cpu().numpy()[rows], exp[rows]), ac
+
+
+def test_bitwise_reproducible():
+    lib().init(0)
+    wl, rl = small_system({0: 2, 1: 1, 2: 1}, 3, 4.0, seed=17)
+    dl = fock.to_device(rl)
+    runs = []
+    for _ in range(2):
+        matJ, matK = fock.build_jk(dl)
+        torch.cuda.synchronize()
+        runs.append(({k: v.cpu().numpy() for k, v in matJ.items()}, {k: v.cpu().numpy() for k, v in matK.items()}))
+    for k in runs[0][0]:
+        assert np.array_equal(runs[0][0][k], runs[1][0][k]), k
+    for k in runs[0][1]:
+        assert np.array_equal(runs[0][1][k], runs[1][1][k]), k
+
+
+def test_quartet_counters_count_screened_work():
+    lib().init(0)
+    wl, rl = small_system({0: 1, 1: 1}, 3, 4.0, seed=19)
+    dl = fock.to_device(rl)
+    L = lib()
+    L.reset_counters()
+    fock.build_jk(dl)
+    c1 = L.quartet_counters(reset=True)
+    fock.build_jk(dl)
+    c2 = L.quartet_counters(reset=True)
+    assert c1 == c2 and c1[0] > 0 and c1[1] > 0
+
+
+def test_edge_cases_empty_and_invalid():
+    lib().init(0)
+    z = tf.load()
+    dl = fixture_lists(z, 1e-12)
+    s = torch.cuda.current_stream().cuda_stream
+    out = torch.zeros(4, dtype=torch.float64, device="cuda")
+    A = fock.coulomb_args(dl, "ssss", out, s)
+    A["ss_prim_pair_count_local"] = 0  # empty bra list: nothing to do
+    lib().coulomb("ssss", A)
+    A = fock.coulomb_args(dl, "ssss", out, s)
+    A["ss_prim_pair_count"] = 0  # empty ket list: J unchanged
+    lib().coulomb("ssss", A)
+    torch.cuda.synchronize()
+    assert float(out.abs().max()) == 0.0
+    # null pointer with a non-zero count is rejected before any launch
+    A = fock.coulomb_args(dl, "ssss", out, s)
+    A["ss_mat_D"] = None
+    rc = getattr(lib().cdll, "vlxb_computeCoulombFockSSSS")(*[A[n] for n in lib().j_params["ssss"]])
+    assert rc == 1
+    # a threshold above every bound screens everything out
+    out2 = torch.zeros(dl.j["ss"]["first"].numel(), dtype=torch.float64, device="cuda")
+    A = fock.coulomb_args(dl, "ssss", out2, s)
+    A["eri_threshold"] = 1e30
+    lib().coulomb("ssss", A)
+    torch.cuda.synchronize()
+    assert float(out2.abs().max()) == 0.0

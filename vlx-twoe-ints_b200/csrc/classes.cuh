@@ -77,7 +77,8 @@ int run_coulomb(const CoulombArgs& a, cudaStream_t st)
     JKetPairs ket{kd.geo, kd.tmax, kd.tmin, kd.Dpp, kd.Dm, kd.Qc, kd.Dc, kd.stride, kd.n};
     int grid = launch_grid_limit();
     if ((int64_t)grid > (int64_t)a.n_ab) grid = (int)a.n_ab;
-    coulomb_kernel<LA, LB, LC, LD><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab);
+    coulomb_kernel<LA, LB, LC, LD><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab,
+                                                                quartet_counters_device());
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }
@@ -130,9 +131,10 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
     KPartnerRecs rcd{gcd.rec_sp, gcd.rec_q, gcd.rec_mask, gcd.seg, gcd.geo, gcd.S, gcd.sp_j, gcd.sp_stride};
     int grid = launch_grid_limit();
     if ((int64_t)grid > (int64_t)a.n_ik) grid = (int)a.n_ik;
+    unsigned long long* qc = quartet_counters_device();
     exchange_kernel<LA, LB, LC, LD><<<grid, K_THREADS, 0, st>>>(out, rab, rcd, a.aoinds[LB], a.count[LB],
                                                                 a.aoinds[LD], a.count[LD], a.D, a.naos, a.maxD,
-                                                                a.omega, a.thr, a.mat_K, tab);
+                                                                a.omega, a.thr, a.mat_K, tab, qc ? qc + 1 : nullptr);
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }

@@ -64,6 +64,10 @@ class Arena {
 // (table upload); call vlxb_init() before any stream capture.
 const double* boys_table_device();
 
+// Per-device counters of screened-in primitive shell quartets processed by
+// the J ([0]) and K ([1]) kernels (device memory, allocated with the table).
+unsigned long long* quartet_counters_device();
+
 // Make the device's default memory pool keep freed scratch (release
 // threshold = max) so per-call scratch costs no new cudaMalloc after warm-up.
 int ensure_pool_configured();

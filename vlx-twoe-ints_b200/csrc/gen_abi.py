@@ -115,7 +115,21 @@ def header():
          "/* Human-readable text for a status code.  No reference counterpart. */",
          "const char* vlxb_status_string(int status);", "",
          "/* ABI version (major * 10000 + minor * 100 + patch).  No reference counterpart. */",
-         "int vlxb_version(void);", ""]
+         "int vlxb_version(void);", "",
+         "/* Schwarz helper for callers that build the lists: for n primitive shell",
+         "   pairs (P[t] of type la, Q[t] of type lb, la <= lb <= 2) writes",
+         "   out[t] = max over components of sqrt|(ab|ab)| / |S_ab|, S_ab the pair",
+         "   prefactor.  The reference's caller computes its Q_ij outside the",
+         "   generator (inputs ab_mat_Q_local, Q_K_ab of gen_coulomb.py:81,",
+         "   gen_exchange.py:92), so this has no counterpart in the reference. */",
+         "int vlxb_schwarzBareMax(int la, int lb, const double* info_a, uint32_t cnt_a, const double* info_b,",
+         "                        uint32_t cnt_b, const uint32_t* P, const uint32_t* Q, uint32_t n, double* out,",
+         "                        void* stream);", "",
+         "/* Screened-in primitive shell quartets processed by the J ([0]) and K ([1])",
+         "   kernels on the current device since the last reset.  Reads into host_out",
+         "   (2 values; synchronises `stream`) when host_out is not NULL, then zeroes",
+         "   the counters when reset != 0.  No reference counterpart. */",
+         "int vlxb_quartetCounters(unsigned long long* host_out, int reset, void* stream);", ""]
     L.append("/* ---- Coulomb: replace computeCoulombFock<ABCD> of gen_coulomb.py:74-93 ---- */")
     for cls in j_classes():
         L.append(f"/* replaces computeCoulombFock{cls.upper()} (gen_coulomb.py:74-93; class list gen_coulomb.py:47-56) */")

@@ -55,7 +55,7 @@ struct JKetPairs {
 template <int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(J_THREADS)
 coulomb_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double thr,
-               const double* __restrict__ boys_tab)
+               const double* __restrict__ boys_tab, unsigned long long* __restrict__ qcount)
 {
     constexpr int L = LA + LB + LC + LD;
     constexpr int NE = nrange(LA, LB), NF = nrange(LC, LD);
@@ -80,6 +80,14 @@ coulomb_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double t
                 else hi = mid;
             }
             s_ncut = lo;
+            // screened-in shell quartets of this record (exact bound, no slack)
+            int lo2 = 0, hi2 = lo;
+            while (lo2 < hi2) {
+                const int mid = (lo2 + hi2) >> 1;
+                if (qb * __ldg(ket.tmax + mid) > thr) lo2 = mid + 1;
+                else hi2 = mid;
+            }
+            if (qcount) atomicAdd(qcount, (unsigned long long)lo2);
         }
         __syncthreads();
         const int ncut = s_ncut;
@@ -167,7 +175,8 @@ exchange_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd,
                 const uint32_t* __restrict__ b_aoinds, uint32_t b_count,
                 const uint32_t* __restrict__ d_aoinds, uint32_t d_count,
                 const double* __restrict__ Dao, uint32_t naos, double maxD, double omega, double thr,
-                double* __restrict__ mat_K, const double* __restrict__ boys_tab)
+                double* __restrict__ mat_K, const double* __restrict__ boys_tab,
+                unsigned long long* __restrict__ qcount)
 {
     constexpr int L = LA + LB + LC + LD;
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
@@ -205,6 +214,7 @@ exchange_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd,
             }
             __syncthreads();
             const int total = s_cnt[nj];
+            if (qcount && threadIdx.x == 0) atomicAdd(qcount, (unsigned long long)total);
             int jj = 0;
             for (int w = threadIdx.x; w < total; w += K_THREADS) {
                 while (s_cnt[jj + 1] <= w) jj++;

@@ -38,6 +38,21 @@ static void build_boys_host(std::vector<double>& tab)
 static std::mutex g_mu;
 static const double* g_boys_dev[64] = {nullptr};
 static bool g_pool_done[64] = {false};
+static unsigned long long* g_counters[64] = {nullptr};
+
+unsigned long long* quartet_counters_device()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_counters[dev]) {
+        unsigned long long* p = nullptr;
+        if (cudaMalloc(&p, 2 * sizeof(unsigned long long)) != cudaSuccess) return nullptr;
+        if (cudaMemset(p, 0, 2 * sizeof(unsigned long long)) != cudaSuccess) return nullptr;
+        g_counters[dev] = p;
+    }
+    return g_counters[dev];
+}
 
 const double* boys_table_device()
 {

@@ -1,0 +1,109 @@
+"""ctypes binding of libvlxb.so (the C ABI declared in include/vlxb.h).
+
+The argument lists are taken from csrc/gen_abi.py, the same generator that
+writes include/vlxb.h and the extern "C" definitions, so the three cannot
+drift apart.  There is no fallback: if the library is missing the import of
+this module's `lib()` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import importlib.util
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(_HERE)
+LIB_PATH = os.path.join(_HERE, "libvlxb.so")
+
+
+class VlxbError(RuntimeError):
+    pass
+
+
+def _load_spec():
+    spec = importlib.util.spec_from_file_location("vlxb_gen_abi", os.path.join(PKG_ROOT, "csrc", "gen_abi.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+ABI = _load_spec()
+
+
+def _ctype(decl: str):
+    t = decl.rsplit(" ", 1)[0]
+    if "*" in t:
+        return ctypes.c_void_p
+    if t.endswith("uint32_t"):
+        return ctypes.c_uint32
+    if t.endswith("double"):
+        return ctypes.c_double
+    if t.endswith("int"):
+        return ctypes.c_int
+    raise ValueError(decl)
+
+
+class Lib:
+    def __init__(self, path: str = LIB_PATH):
+        if not os.path.exists(path):
+            raise VlxbError(f"{path} is missing: build it with `python -m vlxb.build` (nvcc, sm_100a)")
+        self.path = path
+        self.cdll = ctypes.CDLL(path)
+        self.j_params = {}
+        self.k_params = {}
+        for cls in ABI.j_classes():
+            ps = ABI.j_params(cls)
+            f = getattr(self.cdll, f"vlxb_computeCoulombFock{cls.upper()}")
+            f.argtypes = [_ctype(p) for p in ps]
+            f.restype = ctypes.c_int
+            self.j_params[cls] = [ABI.pname(p) for p in ps]
+        for cls in ABI.k_classes():
+            ps = ABI.k_params(cls)
+            f = getattr(self.cdll, f"vlxb_computeExchangeFock{cls.upper()}")
+            f.argtypes = [_ctype(p) for p in ps]
+            f.restype = ctypes.c_int
+            self.k_params[cls] = [ABI.pname(p) for p in ps]
+        c = self.cdll
+        c.vlxb_init.argtypes = [ctypes.c_int]
+        c.vlxb_status_string.restype = ctypes.c_char_p
+        c.vlxb_status_string.argtypes = [ctypes.c_int]
+        c.vlxb_schwarzBareMax.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32,
+                                          ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
+        c.vlxb_quartetCounters.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+
+    def check(self, rc: int, what: str):
+        if rc != 0:
+            raise VlxbError(f"{what}: {self.cdll.vlxb_status_string(rc).decode()} (status {rc})")
+
+    def init(self, device: int):
+        self.check(self.cdll.vlxb_init(int(device)), "vlxb_init")
+
+    def coulomb(self, cls: str, args: dict) -> None:
+        vals = [args[n] for n in self.j_params[cls]]
+        rc = getattr(self.cdll, f"vlxb_computeCoulombFock{cls.upper()}")(*vals)
+        self.check(rc, f"vlxb_computeCoulombFock{cls.upper()}")
+
+    def exchange(self, cls: str, args: dict) -> None:
+        vals = [args[n] for n in self.k_params[cls]]
+        rc = getattr(self.cdll, f"vlxb_computeExchangeFock{cls.upper()}")(*vals)
+        self.check(rc, f"vlxb_computeExchangeFock{cls.upper()}")
+
+    def quartet_counters(self, reset: bool = True, stream: int = 0):
+        out = (ctypes.c_ulonglong * 2)()
+        self.check(self.cdll.vlxb_quartetCounters(ctypes.cast(out, ctypes.c_void_p), int(reset), stream),
+                   "vlxb_quartetCounters")
+        return int(out[0]), int(out[1])
+
+    def reset_counters(self, stream: int = 0):
+        self.check(self.cdll.vlxb_quartetCounters(None, 1, stream), "vlxb_quartetCounters")
+
+
+_LIB = None
+
+
+def lib() -> Lib:
+    global _LIB
+    if _LIB is None:
+        _LIB = Lib()
+    return _LIB

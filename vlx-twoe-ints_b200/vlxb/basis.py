@@ -1,0 +1,196 @@
+"""Synthetic molecules, contracted Cartesian s/p/d basis sets and densities.
+
+This is the caller side of the path (the role VeloxChem's host code plays for
+the reference's emitted kernels): it defines the primitives, the AO map and
+the density that the J/K entry points consume.  The workload recipes are those
+of the benchmark configurations:
+
+  * atoms placed uniformly at random in a cube by rejection sampling with a
+    minimum separation of 1.5 bohr;
+  * per atom, for each shell type, n contracted shells of `degree`
+    primitives; primitive j of shell n has exponent alpha0 * ratio**(degree*n + j)
+    (even-tempered, distinct for every primitive of the atom);
+  * contraction coefficients drawn U(0.2, 1) (seeded), then the contracted
+    function is normalised;
+  * Cartesian d shells; every component of a shell shares the normalisation
+    of its x^l component (so d_xx is unit-normalised, d_xy is not);
+  * density D = C C^T with C ~ N(0,1)^(nao x nocc), orthonormalised in the
+    overlap metric: C <- C (C^T S C)^(-1/2).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+CART = {0: [(0, 0, 0)],
+        1: [(1, 0, 0), (0, 1, 0), (0, 0, 1)],
+        2: [(2, 0, 0), (1, 1, 0), (1, 0, 1), (0, 2, 0), (0, 1, 1), (0, 0, 2)]}
+NCART = {0: 1, 1: 3, 2: 6}
+
+
+def _dfact(n: int) -> float:
+    r = 1.0
+    while n > 1:
+        r *= n
+        n -= 2
+    return r
+
+
+def prim_norm(alpha: float, l: int) -> float:
+    """Normalisation of x^l exp(-alpha r^2)."""
+    return math.sqrt((2.0 * alpha / math.pi) ** 1.5 * (4.0 * alpha) ** l / _dfact(2 * l - 1))
+
+
+@dataclass
+class Shell:
+    atom: int
+    l: int
+    exps: np.ndarray
+    coefs: np.ndarray   # includes primitive and contraction normalisation
+    ao0: int = 0        # first Cartesian AO of the shell
+
+
+@dataclass
+class Molecule:
+    coords: np.ndarray               # (natoms, 3) bohr
+    shells: list = field(default_factory=list)
+    naos: int = 0
+
+    @property
+    def natoms(self):
+        return len(self.coords)
+
+
+def place_atoms(n: int, side: float, rng: np.random.Generator, min_sep: float = 1.5,
+                max_tries: int = 200000) -> np.ndarray:
+    pts = []
+    tries = 0
+    while len(pts) < n:
+        tries += 1
+        if tries > max_tries:
+            raise RuntimeError("could not place atoms with the requested minimum separation")
+        p = rng.uniform(0.0, side, size=3)
+        if all(np.linalg.norm(p - q) >= min_sep for q in pts):
+            pts.append(p)
+    return np.array(pts)
+
+
+def build_molecule(coords: np.ndarray, recipe: dict, degree: int, alpha0: float, ratio: float,
+                   rng: np.random.Generator) -> Molecule:
+    """recipe: {l: number of contracted shells of angular momentum l per atom}."""
+    mol = Molecule(coords=np.asarray(coords, dtype=np.float64))
+    ao = 0
+    for a in range(len(coords)):
+        for l in sorted(recipe):
+            for n in range(recipe[l]):
+                exps = np.array([alpha0 * ratio ** (degree * n + j) for j in range(degree)])
+                c = rng.uniform(0.2, 1.0, size=degree)
+                c = c * np.array([prim_norm(e, l) for e in exps])
+                # normalise the contracted x^l component
+                s = 0.0
+                for i in range(degree):
+                    for j in range(degree):
+                        p = exps[i] + exps[j]
+                        s += c[i] * c[j] * (math.pi / p) ** 1.5 * _dfact(2 * l - 1) / (2.0 * p) ** l
+                c = c / math.sqrt(s)
+                mol.shells.append(Shell(atom=a, l=l, exps=exps, coefs=c, ao0=ao))
+                ao += NCART[l]
+    mol.naos = ao
+    return mol
+
+
+# ------------------------------------------------------------------ overlap
+
+def _overlap_1d(la, lb, PA, PB, p):
+    """Obara-Saika 1D overlap factors s[i][j] (without the prefactor)."""
+    s = np.zeros((la + 1, lb + 1) + np.shape(PA))
+    s[0, 0] = 1.0
+    for i in range(la + 1):
+        for j in range(lb + 1):
+            if i == 0 and j == 0:
+                continue
+            if i > 0:
+                v = PA * s[i - 1, j]
+                if i > 1:
+                    v = v + (i - 1) / (2 * p) * s[i - 2, j]
+                if j > 0:
+                    v = v + j / (2 * p) * s[i - 1, j - 1]
+            else:
+                v = PB * s[i, j - 1]
+                if j > 1:
+                    v = v + (j - 1) / (2 * p) * s[i, j - 2]
+            s[i, j] = v
+    return s
+
+
+def overlap_matrix(mol: Molecule) -> np.ndarray:
+    n = mol.naos
+    S = np.zeros((n, n))
+    for sa in mol.shells:
+        A = mol.coords[sa.atom]
+        for sb in mol.shells:
+            B = mol.coords[sb.atom]
+            ea = sa.exps[:, None]
+            eb = sb.exps[None, :]
+            p = ea + eb
+            P = (ea[..., None] * A + eb[..., None] * B) / p[..., None]
+            K = np.exp(-ea * eb / p * float(np.sum((A - B) ** 2))) * (math.pi / p) ** 1.5
+            cc = sa.coefs[:, None] * sb.coefs[None, :] * K
+            s1 = [_overlap_1d(sa.l, sb.l, P[..., x] - A[x], P[..., x] - B[x], p) for x in range(3)]
+            for ia, (ax, ay, az) in enumerate(CART[sa.l]):
+                for ib, (bx, by, bz) in enumerate(CART[sb.l]):
+                    v = cc * s1[0][ax, bx] * s1[1][ay, by] * s1[2][az, bz]
+                    S[sa.ao0 + ia, sb.ao0 + ib] = v.sum()
+    return S
+
+
+def make_density(mol: Molecule, nocc: int, rng: np.random.Generator, S: np.ndarray | None = None) -> np.ndarray:
+    if S is None:
+        S = overlap_matrix(mol)
+    C = rng.standard_normal((mol.naos, nocc))
+    M = C.T @ S @ C
+    w, V = np.linalg.eigh(M)
+    C = C @ (V @ np.diag(w ** -0.5) @ V.T)
+    return C @ C.T
+
+
+# ------------------------------------------------------------------ configs
+
+@dataclass
+class Workload:
+    name: str
+    mol: Molecule
+    D: np.ndarray
+    threshold: float
+    nocc: int
+
+
+def config_small(seed: int = 0) -> Workload:
+    """5 atoms in a 6-bohr cube, 3s+2p shells of degree 3, alpha = 0.1 * 3^k,
+    10 occupied orbitals, Schwarz threshold 1e-12 (plain FP64 build)."""
+    rng = np.random.default_rng(seed)
+    coords = place_atoms(5, 6.0, rng)
+    mol = build_molecule(coords, {0: 3, 1: 2}, degree=3, alpha0=0.1, ratio=3.0, rng=rng)
+    D = make_density(mol, 10, np.random.default_rng(seed + 1))
+    return Workload("5 atoms 3s2p (45 Cartesian AOs)", mol, D, 1e-12, 10)
+
+
+def config_medium(seed: int = 0) -> Workload:
+    """40 atoms in a 14-bohr cube, 4s+3p+2d shells of degree 3,
+    alpha = 0.05 * 2.5^k, 80 occupied orbitals (1000 Cartesian AOs)."""
+    rng = np.random.default_rng(seed)
+    coords = place_atoms(40, 14.0, rng)
+    mol = build_molecule(coords, {0: 4, 1: 3, 2: 2}, degree=3, alpha0=0.05, ratio=2.5, rng=rng)
+    D = make_density(mol, 80, np.random.default_rng(seed + 1))
+    return Workload("40 atoms 4s3p2d (1000 Cartesian AOs)", mol, D, 1e-12, 80)
+
+
+def config_custom(natoms: int, side: float, recipe: dict, degree: int, alpha0: float, ratio: float,
+                  nocc: int, threshold: float = 1e-12, seed: int = 0) -> Workload:
+    rng = np.random.default_rng(seed)
+    coords = place_atoms(natoms, side, rng)
+    mol = build_molecule(coords, recipe, degree=degree, alpha0=alpha0, ratio=ratio, rng=rng)
+    D = make_density(mol, nocc, np.random.default_rng(seed + 1))
+    return Workload(f"{natoms} atoms custom", mol, D, threshold, nocc)
