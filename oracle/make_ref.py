@@ -92,20 +92,28 @@ def j_unit(cls, expr):
         "    const double* cd_mat_D, const double* ab_mat_Q, const double* cd_mat_Q,",
         "    const uint32_t* ab_first, const uint32_t* ab_second, const double* ab_pdata, uint32_t n_ab,",
         "    const uint32_t* cd_first, const uint32_t* cd_second, const double* cd_pdata, uint32_t n_cd,",
-        "    double eri_threshold, const uint32_t* rows, uint32_t nrows)",
+        "    double eri_threshold, const uint32_t* rows, uint32_t nrows, uint64_t max_eval,",
+        "    uint64_t* cq_pass, uint64_t* cq_eval)",
         "{",
         "    const double* tab = boys_table();",
         "    const int64_t nwork = rows ? (int64_t)nrows : (int64_t)n_ab;",
-        "#pragma omp parallel for schedule(dynamic, 1)",
+        "    uint64_t tot_pass = 0, tot_eval = 0;",
+        "#pragma omp parallel for schedule(dynamic, 1) reduction(+ : tot_pass, tot_eval)",
         "    for (int64_t w = 0; w < nwork; w++) {",
         "        const uint32_t ij = rows ? rows[w] : (uint32_t)w;",
+        "        // passing prefix of the sorted ket list (the emitted kernel's break point)",
+        "        uint32_t lo = 0, hi = n_cd;",
+        "        while (lo < hi) { uint32_t mid = (lo + hi) / 2;",
+        "            if (fabs(ab_mat_Q[ij] * cd_mat_Q[mid] * cd_mat_D[mid]) <= eri_threshold) hi = mid; else lo = mid + 1; }",
+        "        const uint32_t n_eval = (uint64_t)lo < max_eval ? lo : (uint32_t)max_eval;",
+        "        tot_pass += lo; tot_eval += n_eval;",
         "        const uint32_t i = ab_first[ij], j = ab_second[ij];",
         f"        const Prim pi = prim(info[{la}], count[{la}], {la}, i), pj = prim(info[{lb}], count[{lb}], {lb}, j);",
         "        const double a_i = pi.a, a_j = pj.a; const double* r_i = pi.r; const double* r_j = pj.r;",
         "        const double S1 = a_i + a_j, inv_S1 = 1.0 / S1; (void)inv_S1;",
         "        const double S_ij_00 = ab_pdata[ij];",
         "        double J_ij = 0.0;",
-        "        for (uint32_t kl = 0; kl < n_cd; kl++) {",
+        "        for (uint32_t kl = 0; kl < n_eval; kl++) {",
         "            if (fabs(ab_mat_Q[ij] * cd_mat_Q[kl] * cd_mat_D[kl]) <= eri_threshold) break;",
         "            const uint32_t k = cd_first[kl], l = cd_second[kl];",
         f"            const Prim pk = prim(info[{lc}], count[{lc}], {lc}, k), pl = prim(info[{ld}], count[{ld}], {ld}, l);",
@@ -128,6 +136,8 @@ def j_unit(cls, expr):
         "        }",
         "        mat_J[ij] += J_ij;",
         "    }",
+        "    if (cq_pass) *cq_pass = tot_pass;",
+        "    if (cq_eval) *cq_eval = tot_eval;",
         "}",
     ])
     return body
@@ -147,20 +157,31 @@ def k_unit(cls, expr):
         "    const double* Q_ab, const double* Q_cd, const uint32_t* Dinds_ab, const uint32_t* Dinds_cd,",
         "    const uint32_t* displs_ab, const uint32_t* displs_cd, const uint32_t* counts_ab,",
         "    const uint32_t* counts_cd, const double* pdata_ab, const double* pdata_cd,",
-        "    double omega, double eri_threshold, const uint32_t* rows, uint32_t nrows)",
+        "    double omega, double eri_threshold, const uint32_t* rows, uint32_t nrows, uint64_t max_eval,",
+        "    uint64_t* cq_pass, uint64_t* cq_eval)",
         "{",
         "    const double* tab = boys_table();",
         "    const int64_t nwork = rows ? (int64_t)nrows : (int64_t)n_ik;",
-        "#pragma omp parallel for schedule(dynamic, 1)",
+        "    uint64_t tot_pass = 0, tot_eval = 0;",
+        "#pragma omp parallel for schedule(dynamic, 1) reduction(+ : tot_pass, tot_eval)",
         "    for (int64_t w = 0; w < nwork; w++) {",
         "        const uint32_t ik = rows ? rows[w] : (uint32_t)w;",
         "        const uint32_t i = pair_i[ik], k = pair_k[ik];",
         "        const uint32_t count_i = counts_ab[i], count_k = counts_cd[k];",
         "        const uint32_t displ_i = displs_ab[i], displ_k = displs_cd[k];",
+        "        uint64_t row_pass = 0;",
+        "        for (uint32_t j = 0; j < count_i; j++) {",
+        "            uint32_t lo = 0, hi = count_k;",
+        "            while (lo < hi) { uint32_t mid = (lo + hi) / 2;",
+        "                if (fabs(Q_ab[displ_i + j] * Q_cd[displ_k + mid] * bd_max_D) <= eri_threshold) hi = mid; else lo = mid + 1; }",
+        "            row_pass += lo;",
+        "        }",
+        "        uint64_t budget = row_pass < max_eval ? row_pass : max_eval;",
+        "        tot_pass += row_pass; tot_eval += budget;",
         f"        const Prim pi = prim(info[{la}], count[{la}], {la}, i), pk = prim(info[{lc}], count[{lc}], {lc}, k);",
         "        const double a_i = pi.a, a_k = pk.a; const double* r_i = pi.r; const double* r_k = pk.r;",
         "        double K_ik = 0.0;",
-        "        for (uint32_t j = 0; j < count_i; j++) {",
+        "        for (uint32_t j = 0; j < count_i && budget > 0; j++) {",
         "            const double Q_ij = Q_ab[displ_i + j];",
         "            const uint32_t j_prim = Dinds_ab[displ_i + j];",
         f"            const uint32_t j_cgto = aoinds[{lb}][(j_prim / {nb}) + count[{lb}] * (j_prim % {nb})];",
@@ -168,8 +189,9 @@ def k_unit(cls, expr):
         "            const double a_j = pj.a; const double* r_j = pj.r;",
         "            const double S1 = a_i + a_j, inv_S1 = 1.0 / S1; (void)inv_S1;",
         "            const double S_ij_00 = pdata_ab[displ_i + j];",
-        "            for (uint32_t l = 0; l < count_k; l++) {",
+        "            for (uint32_t l = 0; l < count_k && budget > 0; l++) {",
         "                if (fabs(Q_ij * Q_cd[displ_k + l] * bd_max_D) <= eri_threshold) break;",
+        "                budget--;",
         "                const uint32_t l_prim = Dinds_cd[displ_k + l];",
         f"                const uint32_t l_cgto = aoinds[{ld}][(l_prim / {nd}) + count[{ld}] * (l_prim % {nd})];",
         f"                const Prim pl = prim(info[{ld}], count[{ld}], {ld}, l_prim);",
@@ -200,6 +222,8 @@ def k_unit(cls, expr):
         "        }",
         "        mat_K[ik] += K_ik;",
         "    }",
+        "    if (cq_pass) *cq_pass = tot_pass;",
+        "    if (cq_eval) *cq_eval = tot_eval;",
         "}",
     ])
     return body

@@ -4,6 +4,32 @@
 #include "engine.cuh"
 #include "../../include/vlxb.h"
 
+namespace vlxb {
+
+unsigned long long launch_count(bool reset);
+
+// FP64 FMA throughput probe: 8 independent fma chains per thread, iters
+// steps each (2 * 8 * iters flops per thread); out[thread] keeps the result
+// live.  Used to measure the DFMA peak that the roofline divides by.
+__global__ void __launch_bounds__(256) fp64_fma_probe(double* out, int iters)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double a[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = 1.0 + 1e-9 * (t + k);
+    const double b = 0.999999999, c = 1e-9;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) a[k] = fma(a[k], b, c);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += a[k];
+    out[t] = s;
+}
+
+}  // namespace vlxb
+
 extern "C" {
 
 int vlxb_init(int device)
@@ -26,5 +52,20 @@ const char* vlxb_status_string(int status)
 }
 
 int vlxb_version(void) { return 100; }
+
+int vlxb_launchCount(unsigned long long* out, int reset)
+{
+    if (!out) return VLXB_EINVAL;
+    *out = vlxb::launch_count(reset != 0);
+    return VLXB_OK;
+}
+
+int vlxb_fp64Probe(double* out, int iters, int blocks, void* stream)
+{
+    if (!out || iters <= 0 || blocks <= 0) return VLXB_EINVAL;
+    vlxb::fp64_fma_probe<<<blocks, 256, 0, (cudaStream_t)stream>>>(out, iters);
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    return VLXB_OK;
+}
 
 }  // extern "C"

@@ -79,6 +79,7 @@ int run_coulomb(const CoulombArgs& a, cudaStream_t st)
     if ((int64_t)grid > (int64_t)a.n_ab) grid = (int)a.n_ab;
     coulomb_kernel<LA, LB, LC, LD><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab,
                                                                 quartet_counters_device());
+    note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }
@@ -135,6 +136,7 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
     exchange_kernel<LA, LB, LC, LD><<<grid, K_THREADS, 0, st>>>(out, rab, rcd, a.aoinds[LB], a.count[LB],
                                                                 a.aoinds[LD], a.count[LD], a.D, a.naos, a.maxD,
                                                                 a.omega, a.thr, a.mat_K, tab, qc ? qc + 1 : nullptr);
+    note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }

@@ -123,4 +123,8 @@ int kout_prepare(Arena& ar, int na, int nc, int npa, int npc, const uint32_t* pi
 
 int launch_grid_limit();
 
+// Host-side count of this library's own kernel launches (CUB's are not
+// counted); read and reset through vlxb_launchCount.
+void note_launches(int n = 1);
+
 }  // namespace vlxb

@@ -129,7 +129,16 @@ def header():
          "   kernels on the current device since the last reset.  Reads into host_out",
          "   (2 values; synchronises `stream`) when host_out is not NULL, then zeroes",
          "   the counters when reset != 0.  No reference counterpart. */",
-         "int vlxb_quartetCounters(unsigned long long* host_out, int reset, void* stream);", ""]
+         "int vlxb_quartetCounters(unsigned long long* host_out, int reset, void* stream);", "",
+         "/* Number of this library's own kernel launches since the last reset",
+         "   (host-side count; reset != 0 zeroes it after reading).  No reference",
+         "   counterpart. */",
+         "int vlxb_launchCount(unsigned long long* out, int reset);", "",
+         "/* FP64 FMA throughput probe: `blocks` x 256 threads, each running 8",
+         "   independent fma chains of `iters` steps (2*8*iters flops per thread);",
+         "   out needs blocks*256 doubles.  Used by the benchmark to measure the",
+         "   DFMA peak.  No reference counterpart. */",
+         "int vlxb_fp64Probe(double* out, int iters, int blocks, void* stream);", ""]
     L.append("/* ---- Coulomb: replace computeCoulombFock<ABCD> of gen_coulomb.py:74-93 ---- */")
     for cls in j_classes():
         L.append(f"/* replaces computeCoulombFock{cls.upper()} (gen_coulomb.py:74-93; class list gen_coulomb.py:47-56) */")

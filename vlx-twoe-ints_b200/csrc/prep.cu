@@ -2,6 +2,8 @@
 // per-device Boys table and memory-pool set-up.
 #include <cub/cub.cuh>
 #include <math.h>
+
+#include <atomic>
 #include <mutex>
 
 #include "common.cuh"
@@ -87,6 +89,15 @@ int ensure_pool_configured()
     return VLXB_OK;
 }
 
+static std::atomic<unsigned long long> g_launches{0};
+
+void note_launches(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
+
+unsigned long long launch_count(bool reset)
+{
+    return reset ? g_launches.exchange(0) : g_launches.load();
+}
+
 int launch_grid_limit()
 {
     int dev = 0, sms = 148;
@@ -114,6 +125,7 @@ static int finish_grouping(Arena& ar, int64_t ntab, int* table, PairGroups& g)
     int rc = scan_int(ar, table, g.spidx, ntab);
     if (rc) return rc;
     k_scan_total<<<1, 1, 0, st>>>(g.spidx, table, ntab, g.n_sp);
+    note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }
@@ -139,6 +151,7 @@ int group_flat(Arena& ar, int na, int nb, int npa, int npb, const uint32_t* firs
     if (!table) return VLXB_ENOMEM;
     VLXB_CHECK_CUDA(cudaMemsetAsync(table, 0, sizeof(int) * ntab, st));
     k_mark_pairs<<<prep_blocks(n), PREP_THREADS, 0, st>>>(first, second, n, na, nb, npb, table);
+    note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     int rc = finish_grouping(ar, ntab, table, g);
     if (rc) return rc;
@@ -147,8 +160,10 @@ int group_flat(Arena& ar, int na, int nb, int npa, int npb, const uint32_t* firs
     if (rc) return rc;
     k_fill_pairs<<<prep_blocks(n), PREP_THREADS, 0, st>>>(first, second, n, na, nb, npb, g.spidx, g.entry, g.sp_i,
                                                           g.sp_j, g.sp_stride);
+    note_launches();
     k_pair_geo<<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.sp_i, g.sp_j, info_a, cnt_a, info_b,
                                                                    cnt_b, g.geo, g.sp_stride);
+    note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }
@@ -164,6 +179,7 @@ int group_csr(Arena& ar, int na, int nb, int npa, int npb, const uint32_t* displ
     if (!table) return VLXB_ENOMEM;
     VLXB_CHECK_CUDA(cudaMemsetAsync(table, 0, sizeof(int) * ntab, st));
     k_mark_csr<<<prep_blocks(n_first), PREP_THREADS, 0, st>>>(displs, counts, Dinds, n_first, na, nb, npb, table);
+    note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     int rc = finish_grouping(ar, ntab, table, g);
     if (rc) return rc;
@@ -172,8 +188,10 @@ int group_csr(Arena& ar, int na, int nb, int npa, int npb, const uint32_t* displ
     if (rc) return rc;
     k_fill_csr<<<prep_blocks(n_first), PREP_THREADS, 0, st>>>(displs, counts, Dinds, n_first, na, nb, npb, g.spidx,
                                                               g.entry, g.sp_i, g.sp_j, g.sp_stride);
+    note_launches();
     k_pair_geo<<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.sp_i, g.sp_j, info_a, cnt_a, info_b,
                                                                    cnt_b, g.geo, g.sp_stride);
+    note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }
@@ -182,17 +200,20 @@ template <int NXY>
 static void launch_rec_count(const PairGroups& g, const double* Q, int* nrec, cudaStream_t st)
 {
     k_rec_count<NXY><<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, g.sp_stride, Q, nrec);
+    note_launches();
 }
 template <int NXY>
 static void launch_rec_fill(const PairGroups& g, const double* Q, const int* recoff, cudaStream_t st)
 {
     k_rec_fill<NXY><<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, g.sp_stride, Q, recoff,
                                                                        g.rec_sp, g.rec_q, g.rec_mask);
+    note_launches();
 }
 template <int NXY>
 static void launch_sp_S(const PairGroups& g, const double* pdata, cudaStream_t st)
 {
     k_sp_S<NXY><<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, g.sp_stride, pdata, g.S);
+    note_launches();
 }
 
 #define VLXB_NXY_DISPATCH(nxy, FN, ...)            \
@@ -225,6 +246,7 @@ int make_records(Arena& ar, int nxy, PairGroups& g, const double* Q, int64_t n_e
     int rc = scan_int(ar, nrec, recoff, g.sp_stride + 1);
     if (rc) return rc;
     k_scan_total<<<1, 1, 0, st>>>(recoff, nrec, g.sp_stride + 1, g.n_rec);
+    note_launches();
     VLXB_NXY_DISPATCH(nxy, launch_rec_fill, g, Q, recoff, st);
     VLXB_CHECK_CUDA(cudaGetLastError());
     // keep recoff for segment offsets
@@ -245,7 +267,9 @@ int segment_records(Arena& ar, int nxy, int npa, int npb, PairGroups& g, const d
     g.S = ar.alloc<double>(g.sp_stride * nxy);
     if (ar.failed()) return VLXB_ENOMEM;
     k_rec_segments<<<prep_blocks(npa + 1), PREP_THREADS, 0, st>>>(g.spidx, recoff, npa, npb, g.n_rec, seg);
+    note_launches();
     k_iota<<<prep_blocks(g.rec_stride), PREP_THREADS, 0, st>>>(perm_in, g.rec_stride);
+    note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     size_t bytes = 0;
     VLXB_CHECK_CUDA(cub::DeviceSegmentedRadixSort::SortPairsDescending(
@@ -256,6 +280,7 @@ int segment_records(Arena& ar, int nxy, int npa, int npb, PairGroups& g, const d
         tmp, bytes, g.rec_q, q_sorted, perm_in, perm, (int)g.rec_stride, npa, seg, seg + 1, 0, 64, st));
     k_gather_recs<<<prep_blocks(g.rec_stride), PREP_THREADS, 0, st>>>(g.n_rec, perm, g.rec_sp, g.rec_mask,
                                                                        sp_sorted, mask_sorted);
+    note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     g.rec_q = q_sorted;
     g.rec_sp = sp_sorted;
@@ -294,7 +319,9 @@ int jket_prepare(Arena& ar, const PairGroups& g, const uint32_t* first, const ui
     out.n = g.n_sp;
     k_jket_fill<LC, LD><<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, S, first, second, D, Q, pdata,
                                                                  g.geo, keys, tmin_u, Dpp_u, Dm_u, Qc_u, Dc_u, S);
+    note_launches();
     k_iota<<<prep_blocks(S), PREP_THREADS, 0, st>>>(perm_in, S);
+    note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     size_t bytes = 0;
     VLXB_CHECK_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, keys, keys_sorted, perm_in, perm,
@@ -306,6 +333,7 @@ int jket_prepare(Arena& ar, const PairGroups& g, const uint32_t* first, const ui
     k_jket_gather<LC, LD><<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, perm, S, g.geo, keys_sorted, tmin_u,
                                                                    Dpp_u, Dm_u, Qc_u, Dc_u, out.geo, out.tmax,
                                                                    out.tmin, out.Dpp, out.Dm, out.Qc, out.Dc);
+    note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }
@@ -329,6 +357,7 @@ static void launch_kout(const uint32_t* pi, const uint32_t* pk, int64_t n, int n
 {
     k_kout_fill<NAC><<<prep_blocks(n), PREP_THREADS, 0, st>>>(pi, pk, n, na, nc, npc, spidx, out.idx, out.ish,
                                                               out.ksh, out.stride);
+    note_launches();
 }
 
 int kout_prepare(Arena& ar, int na, int nc, int npa, int npc, const uint32_t* pi, const uint32_t* pk, int64_t n,
@@ -340,6 +369,7 @@ int kout_prepare(Arena& ar, int na, int nc, int npa, int npc, const uint32_t* pi
     if (!table) return VLXB_ENOMEM;
     VLXB_CHECK_CUDA(cudaMemsetAsync(table, 0, sizeof(int) * ntab, st));
     k_mark_pairs<<<prep_blocks(n), PREP_THREADS, 0, st>>>(pi, pk, n, na, nc, npc, table);
+    note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     PairGroups g;
     int rc = finish_grouping(ar, ntab, table, g);
