@@ -14,8 +14,7 @@
 
 #include <algorithm>
 #include <functional>
-#include <map>
-#include <utility>
+#include <tuple>
 #include <vector>
 
 namespace {
@@ -24,15 +23,30 @@ inline int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 
 // number of leading entries of a descending array v with pred(v[n]) true
 template <typename F>
-inline int64_t prefix(const std::vector<double>& v, F pred)
+inline int64_t prefix(const double* v, int64_t n, F pred)
 {
-    int64_t lo = 0, hi = (int64_t)v.size();
+    int64_t lo = 0, hi = n;
     while (lo < hi) {
         int64_t mid = (lo + hi) / 2;
         if (pred(v[mid])) lo = mid + 1;
         else hi = mid;
     }
     return lo;
+}
+
+// distinct (key, q) pairs -> per key, the list of distinct q
+struct KeyQ {
+    uint64_t key;
+    double q;
+};
+
+void unique_sorted(std::vector<KeyQ>& v)
+{
+    std::sort(v.begin(), v.end(), [](const KeyQ& a, const KeyQ& b) {
+        return a.key < b.key || (a.key == b.key && a.q < b.q);
+    });
+    v.erase(std::unique(v.begin(), v.end(), [](const KeyQ& a, const KeyQ& b) { return a.key == b.key && a.q == b.q; }),
+            v.end());
 }
 
 }  // namespace
@@ -42,47 +56,54 @@ extern "C" uint64_t vlxref_count_j(int la, int lb, int lc, int ld, const double*
                                    const uint32_t* cd_first, const uint32_t* cd_second, uint32_t n_cd, double thr)
 {
     const int na = ncart(la), nb = ncart(lb), nc = ncart(lc), nd = ncart(ld);
-    std::map<std::pair<uint32_t, uint32_t>, std::vector<double>> bra;
-    for (uint32_t e = 0; e < n_ab; e++) {
-        auto& v = bra[{ab_first[e] / na, ab_second[e] / nb}];
-        if (std::find(v.begin(), v.end(), ab_Q[e]) == v.end()) v.push_back(ab_Q[e]);
-    }
-    std::map<std::pair<uint32_t, uint32_t>, double> ket;
-    for (uint32_t e = 0; e < n_cd; e++) {
-        const double t = fabs(cd_Q[e] * cd_D[e]);
-        auto key = std::make_pair(cd_first[e] / nc, cd_second[e] / nd);
-        auto it = ket.find(key);
-        if (it == ket.end()) ket[key] = t;
-        else it->second = fmax(it->second, t);
-    }
+    std::vector<KeyQ> bra(n_ab);
+    for (uint32_t e = 0; e < n_ab; e++)
+        bra[e] = {((uint64_t)(ab_first[e] / na) << 32) | (ab_second[e] / nb), ab_Q[e]};
+    unique_sorted(bra);
+    std::vector<std::pair<uint64_t, double>> ket(n_cd);
+    for (uint32_t e = 0; e < n_cd; e++)
+        ket[e] = {((uint64_t)(cd_first[e] / nc) << 32) | (cd_second[e] / nd), fabs(cd_Q[e] * cd_D[e])};
+    std::sort(ket.begin(), ket.end());
     std::vector<double> tmax;
-    for (auto& kv : ket) tmax.push_back(kv.second);
+    for (size_t e = 0; e < ket.size();) {
+        size_t f = e;
+        double t = 0.0;
+        while (f < ket.size() && ket[f].first == ket[e].first) t = fmax(t, ket[f++].second);
+        tmax.push_back(t);
+        e = f;
+    }
     std::sort(tmax.begin(), tmax.end(), std::greater<double>());
     uint64_t total = 0;
-    for (auto& kv : bra)
-        for (double q : kv.second) total += (uint64_t)prefix(tmax, [&](double t) { return q * t > thr; });
+#pragma omp parallel for reduction(+ : total)
+    for (int64_t r = 0; r < (int64_t)bra.size(); r++) {
+        const double q = bra[r].q;
+        total += (uint64_t)prefix(tmax.data(), (int64_t)tmax.size(), [&](double t) { return q * t > thr; });
+    }
     return total;
 }
 
-static std::vector<std::vector<double>> partner_records(int lx, int ly, uint32_t nprim_x, const double* Q,
-                                                        const uint32_t* Dinds, const uint32_t* displs,
-                                                        const uint32_t* counts)
+// Records of a CSR partner list grouped by first primitive shell: seg offsets
+// into a flat q array, q descending inside each segment.
+static void partner_records(int lx, int ly, uint32_t nprim_x, const double* Q, const uint32_t* Dinds,
+                            const uint32_t* displs, const uint32_t* counts, std::vector<int64_t>& seg,
+                            std::vector<double>& qs)
 {
     const int nx = ncart(lx), ny = ncart(ly);
-    std::vector<std::map<uint32_t, std::vector<double>>> by(nprim_x);
+    std::vector<std::tuple<uint32_t, uint32_t, double>> v;
     for (uint32_t i = 0; i < nprim_x * (uint32_t)nx; i++)
         for (uint32_t t = 0; t < counts[i]; t++) {
             const uint32_t e = displs[i] + t;
-            auto& v = by[i / nx][Dinds[e] / ny];
-            if (std::find(v.begin(), v.end(), Q[e]) == v.end()) v.push_back(Q[e]);
+            v.emplace_back(i / nx, Dinds[e] / ny, Q[e]);
         }
-    std::vector<std::vector<double>> out(nprim_x);
-    for (uint32_t s = 0; s < nprim_x; s++) {
-        for (auto& kv : by[s])
-            for (double q : kv.second) out[s].push_back(q);
-        std::sort(out[s].begin(), out[s].end(), std::greater<double>());
-    }
-    return out;
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+    seg.assign(nprim_x + 1, 0);
+    for (auto& x : v) seg[std::get<0>(x) + 1]++;
+    for (uint32_t s = 0; s < nprim_x; s++) seg[s + 1] += seg[s];
+    qs.resize(v.size());
+    for (size_t k = 0; k < v.size(); k++) qs[k] = std::get<2>(v[k]);
+    for (uint32_t s = 0; s < nprim_x; s++)
+        std::sort(qs.begin() + seg[s], qs.begin() + seg[s + 1], std::greater<double>());
 }
 
 extern "C" uint64_t vlxref_count_k(int la, int lb, int lc, int ld, uint32_t nprim_a, uint32_t nprim_c,
@@ -92,19 +113,24 @@ extern "C" uint64_t vlxref_count_k(int la, int lb, int lc, int ld, uint32_t npri
                                    const uint32_t* displs_cd, const uint32_t* counts_cd, double maxD, double thr)
 {
     const int na = ncart(la), nc = ncart(lc);
-    auto rab = partner_records(la, lb, nprim_a, Q_ab, Dinds_ab, displs_ab, counts_ab);
-    auto rcd = partner_records(lc, ld, nprim_c, Q_cd, Dinds_cd, displs_cd, counts_cd);
-    std::vector<std::pair<uint32_t, uint32_t>> blocks;
-    blocks.reserve(n_ik);
-    for (uint32_t e = 0; e < n_ik; e++) blocks.push_back({pair_i[e] / na, pair_k[e] / nc});
+    std::vector<int64_t> sa, sc;
+    std::vector<double> qa, qc;
+    partner_records(la, lb, nprim_a, Q_ab, Dinds_ab, displs_ab, counts_ab, sa, qa);
+    partner_records(lc, ld, nprim_c, Q_cd, Dinds_cd, displs_cd, counts_cd, sc, qc);
+    std::vector<uint64_t> blocks(n_ik);
+    for (uint32_t e = 0; e < n_ik; e++) blocks[e] = ((uint64_t)(pair_i[e] / na) << 32) | (pair_k[e] / nc);
     std::sort(blocks.begin(), blocks.end());
     blocks.erase(std::unique(blocks.begin(), blocks.end()), blocks.end());
     uint64_t total = 0;
 #pragma omp parallel for schedule(dynamic, 64) reduction(+ : total)
     for (int64_t b = 0; b < (int64_t)blocks.size(); b++) {
-        const auto& q1s = rab[blocks[b].first];
-        const auto& q2s = rcd[blocks[b].second];
-        for (double q1 : q1s) total += (uint64_t)prefix(q2s, [&](double q2) { return fabs(q1 * q2 * maxD) > thr; });
+        const uint32_t I = (uint32_t)(blocks[b] >> 32), K = (uint32_t)(blocks[b] & 0xffffffffu);
+        const double* q2 = qc.data() + sc[K];
+        const int64_t n2 = sc[K + 1] - sc[K];
+        for (int64_t r = sa[I]; r < sa[I + 1]; r++) {
+            const double q1 = qa[r];
+            total += (uint64_t)prefix(q2, n2, [&](double q) { return fabs(q1 * q * maxD) > thr; });
+        }
     }
     return total;
 }

@@ -223,3 +223,74 @@ def test_edge_cases_empty_and_invalid():
     lib().coulomb("ssss", A)
     torch.cuda.synchronize()
     assert float(out2.abs().max()) == 0.0
+
+
+def _k_variants(cls):
+    """Exchange variants compiled for a class (column ones only when their
+    shared memory fits; the library falls back to the thread kernel)."""
+    import sys as _s
+    import os as _o
+    _s.path.insert(0, _o.path.join(_o.path.dirname(_o.path.dirname(_o.path.abspath(__file__))),
+                                   "vlx-twoe-ints_b200", "csrc"))
+    from gen_column import ColumnPlan, k_smem_bytes
+
+    l = [{"s": 0, "p": 1, "d": 2}[x] for x in cls]
+    out = [0]
+    for ori in (0, 1):
+        if k_smem_bytes(ColumnPlan(*l, ori)) <= 46 * 1024:
+            out.append(1 + ori)
+    return out
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+def test_golden_every_coulomb_variant(golden, variant):
+    """Both Coulomb kernels (thread per quartet, warp column) on every class."""
+    z = golden
+    L = lib()
+    saved = {c: L.get_schedule("J", c) for c in tf.j_classes()}
+    try:
+        for c in tf.j_classes():
+            L.set_schedule("J", c, variant)
+        for tag in ("t12", "t3"):
+            dl = fixture_lists(z, tf.THRESHOLDS[tag])
+            s = torch.cuda.current_stream().cuda_stream
+            bad = []
+            for cls in tf.j_classes():
+                out = torch.zeros(dl.j[cls[:2]]["first"].numel(), dtype=torch.float64, device="cuda")
+                L.coulomb(cls, fock.coulomb_args(dl, cls, out, s))
+                if not close(out.cpu().numpy(), z[f"J_{cls}_{tag}"]):
+                    bad.append(cls)
+            assert not bad, (variant, tag, bad)
+    finally:
+        for c, v in saved.items():
+            L.set_schedule("J", c, v)
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_golden_every_exchange_variant(golden, variant):
+    """All exchange kernels (thread per quartet; column with bra or ket lanes)
+    on every class where the variant is compiled."""
+    z = golden
+    L = lib()
+    saved = {c: L.get_schedule("K", c) for c in tf.k_classes()}
+    try:
+        for c in tf.k_classes():
+            L.set_schedule("K", c, variant if variant in _k_variants(c) else 0)
+        for tag, thr, omega, nrow in tf.K_VARIANTS:
+            dl = fixture_lists(z, thr)
+            s = torch.cuda.current_stream().cuda_stream
+            bad = []
+            for cls in tf.k_classes():
+                ac = cls[0] + cls[2]
+                out = torch.zeros(dl.kpair[ac]["i"].numel(), dtype=torch.float64, device="cuda")
+                L.exchange(cls, fock.exchange_args(dl, cls, out, s, omega))
+                got = out.cpu().numpy()
+                exp = z[f"K_{cls}_{tag}"]
+                if nrow is not None:
+                    got = got[:len(exp)]
+                if not close(got, exp):
+                    bad.append(cls)
+            assert not bad, (variant, tag, bad)
+    finally:
+        for c, v in saved.items():
+            L.set_schedule("K", c, v)

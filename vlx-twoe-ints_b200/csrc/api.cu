@@ -53,6 +53,18 @@ const char* vlxb_status_string(int status)
 
 int vlxb_version(void) { return 100; }
 
+int vlxb_setSchedule(int kind, int la, int lb, int lc, int ld, int variant)
+{
+    return vlxb::schedule_set(kind, la, lb, lc, ld, variant);
+}
+
+int vlxb_getSchedule(int kind, int la, int lb, int lc, int ld)
+{
+    if (kind < 0 || kind > 1 || la < 0 || la > 2 || lb < 0 || lb > 2 || lc < 0 || lc > 2 || ld < 0 || ld > 2)
+        return -VLXB_EINVAL;
+    return vlxb::schedule_get(kind, la, lb, lc, ld);
+}
+
 int vlxb_launchCount(unsigned long long* out, int reset)
 {
     if (!out) return VLXB_EINVAL;

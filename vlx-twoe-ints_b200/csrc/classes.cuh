@@ -1,6 +1,7 @@
 // Per-class host drivers: regroup the caller's lists on the device, then
 // launch the class's integral kernel, all on the caller's stream.
 #pragma once
+#include "col_kernels.cuh"
 #include "engine.cuh"
 #include "jk_kernels.cuh"
 
@@ -77,8 +78,12 @@ int run_coulomb(const CoulombArgs& a, cudaStream_t st)
     JKetPairs ket{kd.geo, kd.tmax, kd.tmin, kd.Dpp, kd.Dm, kd.Qc, kd.Dc, kd.stride, kd.n};
     int grid = launch_grid_limit();
     if ((int64_t)grid > (int64_t)a.n_ab) grid = (int)a.n_ab;
-    coulomb_kernel<LA, LB, LC, LD><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab,
-                                                                quartet_counters_device());
+    if (schedule_get(0, LA, LB, LC, LD) == 1)
+        coulomb_col_kernel<LA, LB, LC, LD><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab,
+                                                                        quartet_counters_device());
+    else
+        coulomb_kernel<LA, LB, LC, LD><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab,
+                                                                    quartet_counters_device());
     note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
@@ -133,9 +138,29 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
     int grid = launch_grid_limit();
     if ((int64_t)grid > (int64_t)a.n_ik) grid = (int)a.n_ik;
     unsigned long long* qc = quartet_counters_device();
-    exchange_kernel<LA, LB, LC, LD><<<grid, K_THREADS, 0, st>>>(out, rab, rcd, a.aoinds[LB], a.count[LB],
-                                                                a.aoinds[LD], a.count[LD], a.D, a.naos, a.maxD,
-                                                                a.omega, a.thr, a.mat_K, tab, qc ? qc + 1 : nullptr);
+    const int var = schedule_get(1, LA, LB, LC, LD);
+    bool launched = false;
+    if constexpr (ColTab<LA, LB, LC, LD, 0>::K_FITS) {
+        if (var == 1) {
+            exchange_col_kernel<LA, LB, LC, LD, 0><<<grid, K_THREADS, 0, st>>>(
+                out, rab, rcd, a.aoinds[LB], a.count[LB], a.aoinds[LD], a.count[LD], a.D, a.naos, a.maxD, a.omega,
+                a.thr, a.mat_K, tab, qc ? qc + 1 : nullptr);
+            launched = true;
+        }
+    }
+    if constexpr (ColTab<LA, LB, LC, LD, 1>::K_FITS) {
+        if (var == 2) {
+            exchange_col_kernel<LA, LB, LC, LD, 1><<<grid, K_THREADS, 0, st>>>(
+                out, rab, rcd, a.aoinds[LB], a.count[LB], a.aoinds[LD], a.count[LD], a.D, a.naos, a.maxD, a.omega,
+                a.thr, a.mat_K, tab, qc ? qc + 1 : nullptr);
+            launched = true;
+        }
+    }
+    if (!launched)
+        exchange_kernel<LA, LB, LC, LD><<<grid, K_THREADS, 0, st>>>(out, rab, rcd, a.aoinds[LB], a.count[LB],
+                                                                    a.aoinds[LD], a.count[LD], a.D, a.naos, a.maxD,
+                                                                    a.omega, a.thr, a.mat_K, tab,
+                                                                    qc ? qc + 1 : nullptr);
     note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;

@@ -1,0 +1,355 @@
+// Warp-cooperative ("column") J and K kernels for the heavy classes (sm_100a).
+//
+// A group of ColTab::NL lanes evaluates one primitive shell quartet: lane x
+// holds the column [x|y]^(m) of its lane-side Cartesian component x in
+// registers, and the step-side components y are built by identical steps on
+// all lanes with one warp shuffle per step for the coupling term (see
+// gen_column.py).  A warp holds ColTab::P such groups.
+//
+// Exchange (ori 0, lanes = bra e; ori 1, lanes = ket f), per quartet:
+//   VRR (column) -> lane-side HRR per lane into shared memory (ori 0: ket
+//   HRR (e|cd); ori 1: bra HRR (ab|f)) -> __syncwarp -> each lane takes fixed
+//   units of the other side (ori 0: cd pairs; ori 1: ab pairs), applies the
+//   remaining HRR and digests into K partials held in registers for the whole
+//   output block.  The block's partials are then reduced in a fixed order.
+// Coulomb (ori 0): lanes accumulate X_e = sum_f (e0|f0) D''_f for their own e
+//   across the bra's kets; the CTA reduces X in a fixed order and applies the
+//   bra HRR once.  No atomics anywhere: results are bit-reproducible.
+#pragma once
+#include "common.cuh"
+#include "jk_kernels.cuh"
+
+namespace vlxb {
+
+template <int LA, int LB, int LC, int LD, int ORI>
+struct ColTab;
+template <int LA, int LB, int LC, int LD, int ORI>
+__device__ __forceinline__ const int8_t* col_tab_ptr();
+
+struct ColLane {
+    int src[3];     // absolute lane owning x - 1_i (self when x_i == 0)
+    double xi[3];   // components of x (coupling multipliers)
+    int cdir[4];    // base-chain directions (-1: inactive step)
+    double ck[4];   // base-chain coefficients
+    int jdir[3];    // level-lam lanes: direction j with x - 1_i = 1_j (-1 otherwise)
+    bool lamlane;   // lane of the lowest lane level when that level derives its partners
+    int tidx;       // index of x among the lane-side targets, -1 if x is a helper
+};
+
+template <int LA, int LB, int LC, int LD, int ORI>
+__device__ __forceinline__ void col_vrr(const QV& q, const double* F, const ColLane& ln, double* out);
+
+template <int LA, int LB, int LC, int LD, int ORI>
+__device__ __forceinline__ ColLane make_lane(int lig, int gbase)
+{
+    const int8_t* r = col_tab_ptr<LA, LB, LC, LD, ORI>() + lig * 20;
+    ColLane ln;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        ln.xi[i] = (double)r[i];
+        ln.src[i] = gbase + r[3 + i];
+        ln.jdir[i] = r[6 + i];
+    }
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+        ln.cdir[s] = r[9 + s];
+        ln.ck[s] = (double)r[13 + s];
+    }
+    ln.lamlane = (r[17] == ColTab<LA, LB, LC, LD, ORI>::LAM) && (r[6] >= 0 || r[7] >= 0 || r[8] >= 0);
+    ln.tidx = r[18];
+    return ln;
+}
+
+// ---------------------------------------------------------------- exchange
+template <int LA, int LB, int LC, int LD, int ORI>
+__global__ void __launch_bounds__(K_THREADS)
+exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd,
+                    const uint32_t* __restrict__ b_aoinds, uint32_t b_count,
+                    const uint32_t* __restrict__ d_aoinds, uint32_t d_count,
+                    const double* __restrict__ Dao, uint32_t naos, double maxD, double omega, double thr,
+                    double* __restrict__ mat_K, const double* __restrict__ boys_tab,
+                    unsigned long long* __restrict__ qcount)
+{
+    using CT = ColTab<LA, LB, LC, LD, ORI>;
+    constexpr int L = LA + LB + LC + LD;
+    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    constexpr int NAC = NA * NC;
+    constexpr int NW = K_THREADS / 32;
+    constexpr int NL = CT::NL, P = CT::P, NXT = CT::NXT, NYT = CT::NYT;
+    // phase-2 units: ori 0 -> cd pairs (accumulate K[a][c(u)]), ori 1 -> ab pairs (K[a(u)][c])
+    constexpr int N2 = ORI == 0 ? NC * ND : NA * NB;
+    constexpr int NACC = ORI == 0 ? NA : NC;
+    constexpr int NPASS = (N2 + NL - 1) / NL;
+    __shared__ double U[NW][P][NXT][N2];
+    __shared__ double red[NW][P][N2][NACC];
+    __shared__ int s_cnt[K_JCHUNK + 1];
+
+    const int nout = *out.n;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane / NL, lig = lane % NL;
+    const bool lane_ok = grp < P;
+    const ColLane ln = make_lane<LA, LB, LC, LD, ORI>(lane_ok ? lig : 0, lane_ok ? grp * NL : lane);
+
+    for (int o = blockIdx.x; o < nout; o += gridDim.x) {
+        const int ish = __ldg(out.ish + o), ksh = __ldg(out.ksh + o);
+        const int a0 = __ldg(ab.seg + ish), a1 = __ldg(ab.seg + ish + 1);
+        const int c0 = __ldg(cd.seg + ksh), c1 = __ldg(cd.seg + ksh + 1);
+        double Kacc[NPASS][NACC];
+#pragma unroll
+        for (int p = 0; p < NPASS; p++)
+#pragma unroll
+            for (int x = 0; x < NACC; x++) Kacc[p][x] = 0.0;
+
+        for (int jb = a0; jb < a1; jb += K_JCHUNK) {
+            const int nj = min(K_JCHUNK, a1 - jb);
+            for (int t = threadIdx.x; t < nj; t += K_THREADS) {
+                const double qij = __ldg(ab.rec_q + jb + t);
+                int lo = c0, hi = c1;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (fabs(qij * __ldg(cd.rec_q + mid) * maxD) > thr) lo = mid + 1;
+                    else hi = mid;
+                }
+                s_cnt[t + 1] = lo - c0;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                s_cnt[0] = 0;
+                for (int t = 1; t <= nj; t++) s_cnt[t] += s_cnt[t - 1];
+            }
+            __syncthreads();
+            const int total = s_cnt[nj];
+            if (qcount && threadIdx.x == 0) atomicAdd(qcount, (unsigned long long)total);
+            const int niter = (total + NW * P - 1) / (NW * P);
+            for (int it = 0; it < niter; it++) {
+                const int w = it * (NW * P) + warp * P + grp;
+                const bool act = lane_ok && w < total;
+                const int wq = act ? w : 0;
+                // j of the flattened (j, l) index: last t with s_cnt[t] <= wq
+                int lo = 0, hi = nj;
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (s_cnt[mid] <= wq) lo = mid;
+                    else hi = mid;
+                }
+                const int jr = jb + lo;
+                const int lr = c0 + (wq - s_cnt[lo]);
+                const int spj = __ldg(ab.rec_sp + jr), spl = __ldg(cd.rec_sp + lr);
+                const PairGeo bg = load_geo(ab.geo, ab.sp_stride, spj);
+                const PairGeo kg = load_geo(cd.geo, cd.sp_stride, spl);
+                QV q;
+                double F[L + 1];
+                make_quartet<L>(bg, kg, omega, boys_tab, q, F);
+                double col[NYT];
+                col_vrr<LA, LB, LC, LD, ORI>(q, F, ln, col);
+                // phase 2a: this lane's HRR over the step side, into shared memory
+                if (lane_ok && ln.tidx >= 0) {
+                    double h[N2];
+                    if (ORI == 0) hrr_bra_vector<LC, LD>(q.CDx, q.CDy, q.CDz, col, h);
+                    else hrr_bra_vector<LA, LB>(q.ABx, q.ABy, q.ABz, col, h);
+#pragma unroll
+                    for (int u = 0; u < N2; u++) U[warp][grp][ln.tidx][u] = h[u];
+                }
+                __syncwarp();
+                // phase 2b: fixed units of the other side per lane
+                if (act) {
+                    const int jsh = __ldg(ab.partner + spj), lsh = __ldg(cd.partner + spl);
+                    const uint64_t mj = __ldg(ab.rec_mask + jr), ml = __ldg(cd.rec_mask + lr);
+#pragma unroll
+                    for (int p = 0; p < NPASS; p++) {
+                        const int u = lig + NL * p;
+                        if (u < N2) {
+                            double v[NXT];
+#pragma unroll
+                            for (int x = 0; x < NXT; x++) v[x] = U[warp][grp][x][u];
+                            if (ORI == 0) {
+                                // unit = (c, d): bra HRR, then K[a][c] += sum_b (ab|cd) Sij[ab] Skl[cd] D[b][d]
+                                const int cc = u / ND, dd = u % ND;
+                                double I[NA * NB];
+                                hrr_bra_vector<LA, LB>(q.ABx, q.ABy, q.ABz, v, I);
+                                const double skl = ((ml >> u) & 1ull) ? __ldg(cd.S + u * cd.sp_stride + spl) : 0.0;
+                                const uint32_t lao = __ldg(d_aoinds + lsh + (int64_t)d_count * dd);
+                                double wv[NB];
+#pragma unroll
+                                for (int b = 0; b < NB; b++) {
+                                    const uint32_t jao = __ldg(b_aoinds + jsh + (int64_t)b_count * b);
+                                    wv[b] = skl * __ldg(Dao + (int64_t)jao * naos + lao);
+                                }
+#pragma unroll
+                                for (int a = 0; a < NA; a++) {
+                                    double s = 0.0;
+#pragma unroll
+                                    for (int b = 0; b < NB; b++) {
+                                        const double sij = ((mj >> (a * NB + b)) & 1ull)
+                                                               ? __ldg(ab.S + (a * NB + b) * ab.sp_stride + spj) : 0.0;
+                                        s = fma(I[a * NB + b] * sij, wv[b], s);
+                                    }
+                                    Kacc[p][a] += s;
+                                }
+                                (void)cc;
+                            } else {
+                                // unit = (a, b): ket HRR, then K[a][c] += Sij[ab] sum_d (ab|cd) Skl[cd] D[b][d]
+                                const int aa = u / NB, bb = u % NB;
+                                double I[NC * ND];
+                                hrr_bra_vector<LC, LD>(q.CDx, q.CDy, q.CDz, v, I);
+                                const double sij = ((mj >> u) & 1ull) ? __ldg(ab.S + u * ab.sp_stride + spj) : 0.0;
+                                const uint32_t jao = __ldg(b_aoinds + jsh + (int64_t)b_count * bb);
+                                double wv[ND];
+#pragma unroll
+                                for (int d = 0; d < ND; d++) {
+                                    const uint32_t lao = __ldg(d_aoinds + lsh + (int64_t)d_count * d);
+                                    wv[d] = sij * __ldg(Dao + (int64_t)jao * naos + lao);
+                                }
+#pragma unroll
+                                for (int c = 0; c < NC; c++) {
+                                    double s = 0.0;
+#pragma unroll
+                                    for (int d = 0; d < ND; d++) {
+                                        const double skl = ((ml >> (c * ND + d)) & 1ull)
+                                                               ? __ldg(cd.S + (c * ND + d) * cd.sp_stride + spl) : 0.0;
+                                        s = fma(I[c * ND + d] * skl, wv[d], s);
+                                    }
+                                    Kacc[p][c] += s;
+                                }
+                                (void)aa;
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            __syncthreads();
+        }
+
+        // fixed-order reduction of the block's partials
+        if (lane_ok) {
+#pragma unroll
+            for (int p = 0; p < NPASS; p++)
+#pragma unroll
+                if (lig + NL * p < N2)
+#pragma unroll
+                    for (int x = 0; x < NACC; x++) red[warp][grp][lig + NL * p][x] = Kacc[p][x];
+        }
+        __syncthreads();
+        if (threadIdx.x < NAC) {
+            const int a = threadIdx.x / NC, c = threadIdx.x % NC;
+            double s = 0.0;
+            for (int w = 0; w < NW; w++)
+                for (int g = 0; g < P; g++) {
+                    if (ORI == 0) {
+                        for (int d = 0; d < ND; d++) s += red[w][g][c * ND + d][a];
+                    } else {
+                        for (int b = 0; b < NB; b++) s += red[w][g][a * NB + b][c];
+                    }
+                }
+            const int32_t pos = __ldg(out.idx + threadIdx.x * out.stride + o);
+            if (pos >= 0) mat_K[pos] += s;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- coulomb
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(J_THREADS)
+coulomb_col_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double thr,
+                   const double* __restrict__ boys_tab, unsigned long long* __restrict__ qcount)
+{
+    using CT = ColTab<LA, LB, LC, LD, 0>;
+    constexpr int L = LA + LB + LC + LD;
+    constexpr int NE = nrange(LA, LB), NF = nrange(LC, LD);
+    constexpr int NAB = ncart(LA) * ncart(LB), NCD = ncart(LC) * ncart(LD);
+    constexpr int NW = J_THREADS / 32;
+    constexpr int NL = CT::NL, P = CT::P;
+    static_assert(CT::NXT == NE && CT::NYT == NF, "column layout");
+    __shared__ double red[NW][P][NE];
+    __shared__ int s_ncut;
+    const int nbra = *bra.n_rec;
+    const int nket = *ket.n;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane / NL, lig = lane % NL;
+    const bool lane_ok = grp < P;
+    const ColLane ln = make_lane<LA, LB, LC, LD, 0>(lane_ok ? lig : 0, lane_ok ? grp * NL : lane);
+
+    for (int r = blockIdx.x; r < nbra; r += gridDim.x) {
+        const int sp = __ldg(bra.rec_sp + r);
+        const PairGeo b = load_geo(bra.geo, bra.sp_stride, sp);
+        const double qb = __ldg(bra.rec_q + r);
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = nket;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (qb * __ldg(ket.tmax + mid) * (1.0 + SCREEN_SLACK) > thr) lo = mid + 1;
+                else hi = mid;
+            }
+            s_ncut = lo;
+            int lo2 = 0, hi2 = lo;
+            while (lo2 < hi2) {
+                const int mid = (lo2 + hi2) >> 1;
+                if (qb * __ldg(ket.tmax + mid) > thr) lo2 = mid + 1;
+                else hi2 = mid;
+            }
+            if (qcount) atomicAdd(qcount, (unsigned long long)lo2);
+        }
+        __syncthreads();
+        const int ncut = s_ncut;
+        double X = 0.0;
+        const int niter = (ncut + NW * P - 1) / (NW * P);
+        for (int it = 0; it < niter; it++) {
+            const int kt0 = it * (NW * P) + warp * P + grp;
+            const bool act = lane_ok && kt0 < ncut;
+            const int kt = act ? kt0 : 0;
+            const PairGeo k = load_geo(ket.geo, ket.stride, kt);
+            QV q;
+            double F[L + 1];
+            make_quartet<L>(b, k, 0.0, boys_tab, q, F);
+            double col[NF];
+            col_vrr<LA, LB, LC, LD, 0>(q, F, ln, col);
+            if (act && ln.tidx >= 0) {
+                double Dpp[NF];
+                if (qb * __ldg(ket.tmin + kt) > thr * (1.0 + SCREEN_SLACK)) {
+#pragma unroll
+                    for (int f = 0; f < NF; f++) Dpp[f] = __ldg(ket.Dpp + f * ket.stride + kt);
+                } else {
+                    double Dm[NCD];
+#pragma unroll
+                    for (int c = 0; c < NCD; c++) {
+                        const double qk = __ldg(ket.Qc + c * ket.stride + kt);
+                        const double dk = __ldg(ket.Dc + c * ket.stride + kt);
+                        Dm[c] = (fabs(qb * qk * dk) > thr) ? __ldg(ket.Dm + c * ket.stride + kt) : 0.0;
+                    }
+                    hrr_ket_adjoint<LC, LD>(k.Rx, k.Ry, k.Rz, Dm, Dpp);
+                }
+                double s = 0.0;
+#pragma unroll
+                for (int f = 0; f < NF; f++) s = fma(col[f], Dpp[f], s);
+                X += s;
+            }
+        }
+        if (lane_ok && ln.tidx >= 0) red[warp][grp][ln.tidx] = X;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double Xs[NE];
+#pragma unroll
+            for (int e = 0; e < NE; e++) {
+                double s = 0.0;
+                for (int w = 0; w < NW; w++)
+                    for (int g = 0; g < P; g++) s += red[w][g][e];
+                Xs[e] = s;
+            }
+            double J[NAB];
+            hrr_bra_vector<LA, LB>(b.Rx, b.Ry, b.Rz, Xs, J);
+            const uint64_t mask = __ldg(bra.rec_mask + r);
+#pragma unroll
+            for (int c = 0; c < NAB; c++) {
+                if ((mask >> c) & 1ull) {
+                    const int32_t o = __ldg(bra.entry + c * bra.sp_stride + sp);
+                    mat_J[o] += __ldg(bra.pdata + o) * J[c];
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace vlxb

@@ -123,6 +123,13 @@ int kout_prepare(Arena& ar, int na, int nc, int npa, int npc, const uint32_t* pi
 
 int launch_grid_limit();
 
+// Kernel variant per class: kind 0 = Coulomb (0 thread-per-quartet, 1 column),
+// kind 1 = exchange (0 thread-per-quartet, 1 column with bra lanes, 2 column
+// with ket lanes).  Defaults come from the generator; the autotuner
+// overrides them through vlxb_setSchedule.
+int schedule_get(int kind, int la, int lb, int lc, int ld);
+int schedule_set(int kind, int la, int lb, int lc, int ld, int variant);
+
 // Host-side count of this library's own kernel launches (CUB's are not
 // counted); read and reset through vlxb_launchCount.
 void note_launches(int n = 1);

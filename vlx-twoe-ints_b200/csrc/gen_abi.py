@@ -138,7 +138,15 @@ def header():
          "   independent fma chains of `iters` steps (2*8*iters flops per thread);",
          "   out needs blocks*256 doubles.  Used by the benchmark to measure the",
          "   DFMA peak.  No reference counterpart. */",
-         "int vlxb_fp64Probe(double* out, int iters, int blocks, void* stream);", ""]
+         "int vlxb_fp64Probe(double* out, int iters, int blocks, void* stream);", "",
+         "/* Kernel variant used for one class (kind 0 = Coulomb: 0 one thread per",
+         "   shell quartet, 1 warp-cooperative column kernel; kind 1 = exchange: 0",
+         "   one thread per quartet, 1 column kernel with bra lanes, 2 column kernel",
+         "   with ket lanes).  Every variant gives the same J/K to rounding; the",
+         "   choice only changes speed.  Set by the autotuner.  No reference",
+         "   counterpart. */",
+         "int vlxb_setSchedule(int kind, int la, int lb, int lc, int ld, int variant);",
+         "int vlxb_getSchedule(int kind, int la, int lb, int lc, int ld);", ""]
     L.append("/* ---- Coulomb: replace computeCoulombFock<ABCD> of gen_coulomb.py:74-93 ---- */")
     for cls in j_classes():
         L.append(f"/* replaces computeCoulombFock{cls.upper()} (gen_coulomb.py:74-93; class list gen_coulomb.py:47-56) */")
@@ -216,6 +224,8 @@ def class_tu(cls, kind):
          '#include "../common.cuh"',
          f'#include "q_{cls}.cuh"',
          '#include "hrr_pairs.cuh"',
+         '#include "../col_kernels.cuh"',
+         f'#include "col_{cls}.cuh"',
          '#include "../classes.cuh"', "",
          "namespace vlxb {"]
     if kind == "j":

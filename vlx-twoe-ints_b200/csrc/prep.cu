@@ -89,6 +89,35 @@ int ensure_pool_configured()
     return VLXB_OK;
 }
 
+#include "generated/schedule_default.inc"
+
+static std::atomic<int> g_sched[2][81];
+static std::once_flag g_sched_once;
+
+static void sched_init()
+{
+    for (int c = 0; c < 81; c++) {
+        g_sched[0][c].store(kDefaultScheduleJ[c]);
+        g_sched[1][c].store(kDefaultScheduleK[c]);
+    }
+}
+
+int schedule_get(int kind, int la, int lb, int lc, int ld)
+{
+    std::call_once(g_sched_once, sched_init);
+    return g_sched[kind & 1][la * 27 + lb * 9 + lc * 3 + ld].load(std::memory_order_relaxed);
+}
+
+int schedule_set(int kind, int la, int lb, int lc, int ld, int variant)
+{
+    if (kind < 0 || kind > 1 || la < 0 || la > 2 || lb < 0 || lb > 2 || lc < 0 || lc > 2 || ld < 0 || ld > 2)
+        return VLXB_EINVAL;
+    if (variant < 0 || variant > (kind == 0 ? 1 : 2)) return VLXB_EINVAL;
+    std::call_once(g_sched_once, sched_init);
+    g_sched[kind][la * 27 + lb * 9 + lc * 3 + ld].store(variant);
+    return VLXB_OK;
+}
+
 static std::atomic<unsigned long long> g_launches{0};
 
 void note_launches(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }

@@ -71,6 +71,10 @@ class Lib:
                                           ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                           ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
         c.vlxb_quartetCounters.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        c.vlxb_setSchedule.argtypes = [ctypes.c_int] * 6
+        c.vlxb_getSchedule.argtypes = [ctypes.c_int] * 5
+        c.vlxb_launchCount.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        c.vlxb_fp64Probe.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
 
     def check(self, rc: int, what: str):
         if rc != 0:
@@ -94,6 +98,20 @@ class Lib:
         self.check(self.cdll.vlxb_quartetCounters(ctypes.cast(out, ctypes.c_void_p), int(reset), stream),
                    "vlxb_quartetCounters")
         return int(out[0]), int(out[1])
+
+    def set_schedule(self, kind: str, cls: str, variant: int):
+        """kind "J" or "K"; cls like "pdpd"; see include/vlxb.h for variants."""
+        l = [{"s": 0, "p": 1, "d": 2}[x] for x in cls]
+        self.check(self.cdll.vlxb_setSchedule(0 if kind == "J" else 1, *l, int(variant)), "vlxb_setSchedule")
+
+    def get_schedule(self, kind: str, cls: str) -> int:
+        l = [{"s": 0, "p": 1, "d": 2}[x] for x in cls]
+        return int(self.cdll.vlxb_getSchedule(0 if kind == "J" else 1, *l))
+
+    def launch_count(self, reset: bool = False) -> int:
+        out = ctypes.c_ulonglong(0)
+        self.check(self.cdll.vlxb_launchCount(ctypes.byref(out), int(reset)), "vlxb_launchCount")
+        return int(out.value)
 
     def reset_counters(self, stream: int = 0):
         self.check(self.cdll.vlxb_quartetCounters(None, 1, stream), "vlxb_quartetCounters")

@@ -28,11 +28,12 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v", "-I", CSRC] + ARCH_FLAGS
 
-COMMON_HEADERS = ["common.cuh", "engine.cuh", "jk_kernels.cuh", "prep.cuh", "classes.cuh"]
+COMMON_HEADERS = ["common.cuh", "engine.cuh", "jk_kernels.cuh", "prep.cuh", "classes.cuh", "col_kernels.cuh"]
 
 
 def _run_generators():
     subprocess.run([sys.executable, os.path.join(CSRC, "gen_quartets.py"), GEN], check=True)
+    subprocess.run([sys.executable, os.path.join(CSRC, "gen_column.py"), GEN], check=True)
     subprocess.run([sys.executable, os.path.join(CSRC, "gen_abi.py")], check=True)
 
 
@@ -48,7 +49,10 @@ def _deps(src):
                                                                      os.path.join(REPO_ROOT, "include", "vlxb.h")]
     base = os.path.basename(src)
     if base.startswith("cls_"):
+        deps.append(os.path.join(GEN, f"col_{base.split('_')[1]}.cuh"))
         deps.append(os.path.join(GEN, f"q_{base.split('_')[1]}.cuh"))
+    if base == "prep.cu":
+        deps.append(os.path.join(GEN, "schedule_default.inc"))
     return deps
 
 
