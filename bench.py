@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--fp32-cut", type=float, default=1e-6,
+                    help="mixed-precision leg: quartets with bound below this run in FP32 (0 skips the leg)")
+    ap.add_argument("--schedule", default=None, help="kernel schedule JSON (default: vlxb/schedule_b200.json)")
     return ap.parse_args()
 
 
@@ -287,6 +290,10 @@ def run_ours(args):
 
     L = lib()
     L.init(local)
+    from vlxb.tune import DEFAULT_SCHEDULE, apply_schedule
+
+    sched_loaded = apply_schedule(args.schedule or DEFAULT_SCHEDULE)
+    L.set_fp32_cut(0.0)
     stream = torch.cuda.Stream(device=dev)
     wl = workload(args.config)
     rl = lists.build_lists(wl.mol, wl.D, wl.threshold, fock.gpu_schwarz_fn(dev))
@@ -378,6 +385,38 @@ def run_ours(args):
                 per_class.append((kind, cls, e0.elapsed_time(e1) / 1e3, nq, nq * fl[cls][kind]))
         peak = fp64_peak(L, dev, stream)
 
+        # ---- mixed precision leg: same build with FP32 below the cutoff,
+        # errors of AO J, K and E against this GPU's FP64 build
+        mixed = None
+        if args.fp32_cut > 0:
+            zero_outputs()
+            fock.build_jk(dl, stream=stream, matJ=matJ, matK=matK)
+            torch.cuda.synchronize()
+            J64 = lists.contract_J(rl, {k: v.cpu().numpy() for k, v in matJ.items()})
+            K64 = lists.contract_K(rl, {k: v.cpu().numpy() for k, v in matK.items()})
+            L.set_fp32_cut(args.fp32_cut)
+            one_build()
+            torch.cuda.synchronize()
+            mt = []
+            for _ in range(args.steps):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                one_build()
+                e1.record(stream)
+                e1.synchronize()
+                mt.append(e0.elapsed_time(e1) / 1e3)
+            L.set_fp32_cut(0.0)
+            J32 = lists.contract_J(rl, {k: v.cpu().numpy() for k, v in matJ.items()})
+            K32 = lists.contract_K(rl, {k: v.cpu().numpy() for k, v in matK.items()})
+            t_mix = dist_max(sum(mt)) / len(mt)
+            mixed = {"fp32_below_bound": args.fp32_cut, "value": qpb / t_mix * ws, "unit": UNIT,
+                     "ms_per_step": t_mix * 1e3, "builds_per_s": ws / t_mix,
+                     "speedup_vs_fp64": t_build / t_mix,
+                     "max_abs_dJ": float(np.abs(J32 - J64).max()), "max_abs_dK": float(np.abs(K32 - K64).max()),
+                     "abs_dE_Eh": abs(lists.energy(wl.D, J32, K32) - lists.energy(wl.D, J64, K64)),
+                     "reference": "this GPU's FP64 build (parity-tested against the FP64 oracle at 1e-10)"}
+
     dom = max(per_class, key=lambda r: r[2])
     total_flops = sum(r[4] for r in per_class)
     total_t = sum(r[2] for r in per_class)
@@ -397,7 +436,8 @@ def run_ours(args):
         "builds_per_s": ws / t_build, "quartets_per_build": qpb, "gpu_launches": launches,
         "e2e": {"value": qpb / t_e2e * ws, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": t_e2e * 1e3},
-        "roofline": roofline, "clocks": clk,
+        "roofline": roofline, "clocks": clk, "mixed": mixed,
+        "schedule": "autotuned (vlxb/schedule_b200.json)" if sched_loaded else "generator defaults",
         "top_classes": [{"class": f"{k} {c.upper()}", "ms": round(t * 1e3, 2), "quartets": n,
                          "tflops": round(f / t / 1e12, 3)} for k, c, t, n, f in
                         sorted(per_class, key=lambda r: -r[2])[:8]],

@@ -294,3 +294,34 @@ def test_golden_every_exchange_variant(golden, variant):
     finally:
         for c, v in saved.items():
             L.set_schedule("K", c, v)
+
+
+def test_mixed_precision_errors_within_tolerance():
+    """FP32 below a Schwarz bound of 1e-6, FP64 above and for all accumulation:
+    AO J and K within 1e-7 and E within 1e-6 Eh of the FP64 oracle."""
+    lib().init(0)
+    wl, rl = small_system({0: 2, 1: 1, 2: 1}, 3, 4.0, seed=29)
+    dl = fock.to_device(rl)
+    L = lib()
+    try:
+        L.set_fp32_cut(1e-6)
+        matJ, matK = fock.build_jk(dl)
+        torch.cuda.synchronize()
+    finally:
+        L.set_fp32_cut(0.0)
+    oJ, oK = helpers.oracle_jk_all(rl)
+    J = lists.contract_J(rl, {k: v.cpu().numpy() for k, v in matJ.items()})
+    K = lists.contract_K(rl, {k: v.cpu().numpy() for k, v in matK.items()})
+    Jo, Ko = lists.contract_J(rl, oJ), lists.contract_K(rl, oK)
+    assert np.abs(J - Jo).max() <= 1e-7
+    assert np.abs(K - Ko).max() <= 1e-7
+    assert abs(lists.energy(wl.D, J, K) - lists.energy(wl.D, Jo, Ko)) <= 1e-6
+    # a cutoff above every bound runs everything in FP32: still close, not exact
+    try:
+        L.set_fp32_cut(1e30)
+        mJ, mK = fock.build_jk(dl)
+        torch.cuda.synchronize()
+    finally:
+        L.set_fp32_cut(0.0)
+    J2 = lists.contract_J(rl, {k: v.cpu().numpy() for k, v in mJ.items()})
+    assert np.abs(J2 - Jo).max() <= 1e-4 * np.abs(Jo).max()

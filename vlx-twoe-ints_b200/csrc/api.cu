@@ -37,8 +37,13 @@ int vlxb_init(int device)
     if (cudaSetDevice(device) != cudaSuccess) return VLXB_ECUDA;
     int rc = vlxb::ensure_pool_configured();
     if (rc) return rc;
-    return vlxb::boys_table_device() ? VLXB_OK : VLXB_ECUDA;
+    if (!vlxb::quartet_counters_device()) return VLXB_ECUDA;
+    return (vlxb::boys_table_device() && vlxb::boys_table32_device()) ? VLXB_OK : VLXB_ECUDA;
 }
+
+int vlxb_setFp32Cutoff(double cutoff) { return vlxb::fp32_cut_set(cutoff); }
+
+double vlxb_getFp32Cutoff(void) { return vlxb::fp32_cut_get(); }
 
 const char* vlxb_status_string(int status)
 {

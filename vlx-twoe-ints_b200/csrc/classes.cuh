@@ -58,8 +58,9 @@ int run_coulomb(const CoulombArgs& a, cudaStream_t st)
     if (!(a.thr >= 0.0)) return VLXB_EINVAL;
     int rc = ensure_pool_configured();
     if (rc) return rc;
-    const double* tab = boys_table_device();
-    if (!tab) return VLXB_ECUDA;
+    const BoysTabs tab{boys_table_device(), boys_table32_device()};
+    if (!tab.f64 || !tab.f32) return VLXB_ECUDA;
+    const double cut = fp32_cut_get();
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     Arena ar(st);
     PairGroups gb, gk;
@@ -80,10 +81,10 @@ int run_coulomb(const CoulombArgs& a, cudaStream_t st)
     if ((int64_t)grid > (int64_t)a.n_ab) grid = (int)a.n_ab;
     if (schedule_get(0, LA, LB, LC, LD) == 1)
         coulomb_col_kernel<LA, LB, LC, LD><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab,
-                                                                        quartet_counters_device());
+                                                                        quartet_counters_device(), cut);
     else
         coulomb_kernel<LA, LB, LC, LD><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab,
-                                                                    quartet_counters_device());
+                                                                    quartet_counters_device(), cut);
     note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
@@ -102,8 +103,9 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
     if (!(a.thr >= 0.0) || !(a.omega >= 0.0)) return VLXB_EINVAL;
     int rc = ensure_pool_configured();
     if (rc) return rc;
-    const double* tab = boys_table_device();
-    if (!tab) return VLXB_ECUDA;
+    const BoysTabs tab{boys_table_device(), boys_table32_device()};
+    if (!tab.f64 || !tab.f32) return VLXB_ECUDA;
+    const double cut = fp32_cut_get();
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     Arena ar(st);
     KOutData ko;
@@ -138,29 +140,27 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
     int grid = launch_grid_limit();
     if ((int64_t)grid > (int64_t)a.n_ik) grid = (int)a.n_ik;
     unsigned long long* qc = quartet_counters_device();
+    unsigned long long* qk = qc ? qc + 1 : nullptr;
+    const KDensity dm{a.aoinds[LB], a.count[LB], a.aoinds[LD], a.count[LD], a.D, a.naos};
     const int var = schedule_get(1, LA, LB, LC, LD);
     bool launched = false;
     if constexpr (ColTab<LA, LB, LC, LD, 0>::K_FITS) {
         if (var == 1) {
-            exchange_col_kernel<LA, LB, LC, LD, 0><<<grid, K_THREADS, 0, st>>>(
-                out, rab, rcd, a.aoinds[LB], a.count[LB], a.aoinds[LD], a.count[LD], a.D, a.naos, a.maxD, a.omega,
-                a.thr, a.mat_K, tab, qc ? qc + 1 : nullptr);
+            exchange_col_kernel<LA, LB, LC, LD, 0><<<grid, K_THREADS, 0, st>>>(out, rab, rcd, dm, a.maxD, a.omega,
+                                                                                a.thr, a.mat_K, tab, qk, cut);
             launched = true;
         }
     }
     if constexpr (ColTab<LA, LB, LC, LD, 1>::K_FITS) {
         if (var == 2) {
-            exchange_col_kernel<LA, LB, LC, LD, 1><<<grid, K_THREADS, 0, st>>>(
-                out, rab, rcd, a.aoinds[LB], a.count[LB], a.aoinds[LD], a.count[LD], a.D, a.naos, a.maxD, a.omega,
-                a.thr, a.mat_K, tab, qc ? qc + 1 : nullptr);
+            exchange_col_kernel<LA, LB, LC, LD, 1><<<grid, K_THREADS, 0, st>>>(out, rab, rcd, dm, a.maxD, a.omega,
+                                                                                a.thr, a.mat_K, tab, qk, cut);
             launched = true;
         }
     }
     if (!launched)
-        exchange_kernel<LA, LB, LC, LD><<<grid, K_THREADS, 0, st>>>(out, rab, rcd, a.aoinds[LB], a.count[LB],
-                                                                    a.aoinds[LD], a.count[LD], a.D, a.naos, a.maxD,
-                                                                    a.omega, a.thr, a.mat_K, tab,
-                                                                    qc ? qc + 1 : nullptr);
+        exchange_kernel<LA, LB, LC, LD><<<grid, K_THREADS, 0, st>>>(out, rab, rcd, dm, a.maxD, a.omega, a.thr,
+                                                                    a.mat_K, tab, qk, cut);
     note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;

@@ -15,6 +15,8 @@
 // Coulomb (ori 0): lanes accumulate X_e = sum_f (e0|f0) D''_f for their own e
 //   across the bra's kets; the CTA reduces X in a fixed order and applies the
 //   bra HRR once.  No atomics anywhere: results are bit-reproducible.
+// Mixed precision as in jk_kernels.cuh: quartets below fp32_cut run the same
+// column code in FP32 with FP64 accumulation.
 #pragma once
 #include "common.cuh"
 #include "jk_kernels.cuh"
@@ -36,8 +38,8 @@ struct ColLane {
     int tidx;       // index of x among the lane-side targets, -1 if x is a helper
 };
 
-template <int LA, int LB, int LC, int LD, int ORI>
-__device__ __forceinline__ void col_vrr(const QV& q, const double* F, const ColLane& ln, double* out);
+template <int LA, int LB, int LC, int LD, int ORI, typename T>
+__device__ __forceinline__ void col_vrr(const QVT<T>& q, const T* F, const ColLane& ln, T* out);
 
 template <int LA, int LB, int LC, int LD, int ORI>
 __device__ __forceinline__ ColLane make_lane(int lig, int gbase)
@@ -62,32 +64,132 @@ __device__ __forceinline__ ColLane make_lane(int lig, int gbase)
 
 // ---------------------------------------------------------------- exchange
 template <int LA, int LB, int LC, int LD, int ORI>
-__global__ void __launch_bounds__(K_THREADS)
-exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd,
-                    const uint32_t* __restrict__ b_aoinds, uint32_t b_count,
-                    const uint32_t* __restrict__ d_aoinds, uint32_t d_count,
-                    const double* __restrict__ Dao, uint32_t naos, double maxD, double omega, double thr,
-                    double* __restrict__ mat_K, const double* __restrict__ boys_tab,
-                    unsigned long long* __restrict__ qcount)
-{
+struct KColShape {
     using CT = ColTab<LA, LB, LC, LD, ORI>;
+    static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    static constexpr int NL = CT::NL, P = CT::P, NXT = CT::NXT, NYT = CT::NYT;
+    // phase-2 units: ori 0 -> cd pairs (accumulate K[a][c(u)]), ori 1 -> ab pairs (K[a(u)][c])
+    static constexpr int N2 = ORI == 0 ? NC * ND : NA * NB;
+    static constexpr int NACC = ORI == 0 ? NA : NC;
+    static constexpr int NPASS = (N2 + NL - 1) / NL;
+};
+
+template <int LA, int LB, int LC, int LD, int ORI, typename T>
+__device__ __forceinline__ void kcol_quartet(bool act, int jr, int lr, const KPartnerRecs& ab,
+                                             const KPartnerRecs& cd, const KDensity& dm, double omega,
+                                             const BoysTabs& tabs, const ColLane& ln, bool lane_ok, int lig,
+                                             double (*U)[KColShape<LA, LB, LC, LD, ORI>::N2],
+                                             double (*Kacc)[KColShape<LA, LB, LC, LD, ORI>::NACC])
+{
+    using S = KColShape<LA, LB, LC, LD, ORI>;
     constexpr int L = LA + LB + LC + LD;
-    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND;
+    constexpr int NL = S::NL, NXT = S::NXT, NYT = S::NYT, N2 = S::N2, NPASS = S::NPASS;
+    const int spj = __ldg(ab.rec_sp + jr), spl = __ldg(cd.rec_sp + lr);
+    const PairGeo bg = load_geo(ab.geo, ab.sp_stride, spj);
+    const PairGeo kg = load_geo(cd.geo, cd.sp_stride, spl);
+    QVT<T> q;
+    T F[L + 1];
+    make_quartet_t<L>(bg, kg, omega, tabs.f64, tabs.f32, q, F);
+    T col[NYT];
+    col_vrr<LA, LB, LC, LD, ORI, T>(q, F, ln, col);
+    // phase 2a: this lane's HRR over the step side, into shared memory
+    if (lane_ok && ln.tidx >= 0) {
+        T h[N2];
+        if (ORI == 0) hrr_bra_vector<LC, LD, T>(q.CDx, q.CDy, q.CDz, col, h);
+        else hrr_bra_vector<LA, LB, T>(q.ABx, q.ABy, q.ABz, col, h);
+#pragma unroll
+        for (int u = 0; u < N2; u++) U[ln.tidx][u] = (double)h[u];
+    }
+    __syncwarp();
+    // phase 2b: fixed units of the other side per lane
+    if (act) {
+        const int jsh = __ldg(ab.partner + spj), lsh = __ldg(cd.partner + spl);
+        const uint64_t mj = __ldg(ab.rec_mask + jr), ml = __ldg(cd.rec_mask + lr);
+#pragma unroll
+        for (int p = 0; p < NPASS; p++) {
+            const int u = lig + NL * p;
+            if (u < N2) {
+                T v[NXT];
+#pragma unroll
+                for (int x = 0; x < NXT; x++) v[x] = (T)U[x][u];
+                if (ORI == 0) {
+                    // unit = (c, d): bra HRR, then K[a][c] += sum_b (ab|cd) Sij[ab] Skl[cd] D[b][d]
+                    const int dd = u % ND;
+                    T I[NA * NB];
+                    hrr_bra_vector<LA, LB, T>(q.ABx, q.ABy, q.ABz, v, I);
+                    const double skl = ((ml >> u) & 1ull) ? __ldg(cd.S + u * cd.sp_stride + spl) : 0.0;
+                    const uint32_t lao = __ldg(dm.d_aoinds + lsh + (int64_t)dm.d_count * dd);
+                    T wv[NB];
+#pragma unroll
+                    for (int b = 0; b < NB; b++) {
+                        const uint32_t jao = __ldg(dm.b_aoinds + jsh + (int64_t)dm.b_count * b);
+                        wv[b] = (T)(skl * __ldg(dm.D + (int64_t)jao * dm.naos + lao));
+                    }
+#pragma unroll
+                    for (int a = 0; a < NA; a++) {
+                        T s = (T)0;
+#pragma unroll
+                        for (int b = 0; b < NB; b++) {
+                            const T sij = ((mj >> (a * NB + b)) & 1ull)
+                                              ? (T)__ldg(ab.S + (a * NB + b) * ab.sp_stride + spj) : (T)0;
+                            s = fma(I[a * NB + b] * sij, wv[b], s);
+                        }
+                        Kacc[p][a] += (double)s;
+                    }
+                } else {
+                    // unit = (a, b): ket HRR, then K[a][c] += Sij[ab] sum_d (ab|cd) Skl[cd] D[b][d]
+                    const int bb = u % NB;
+                    T I[NC * ND];
+                    hrr_bra_vector<LC, LD, T>(q.CDx, q.CDy, q.CDz, v, I);
+                    const double sij = ((mj >> u) & 1ull) ? __ldg(ab.S + u * ab.sp_stride + spj) : 0.0;
+                    const uint32_t jao = __ldg(dm.b_aoinds + jsh + (int64_t)dm.b_count * bb);
+                    T wv[ND];
+#pragma unroll
+                    for (int d = 0; d < ND; d++) {
+                        const uint32_t lao = __ldg(dm.d_aoinds + lsh + (int64_t)dm.d_count * d);
+                        wv[d] = (T)(sij * __ldg(dm.D + (int64_t)jao * dm.naos + lao));
+                    }
+#pragma unroll
+                    for (int c = 0; c < NC; c++) {
+                        T s = (T)0;
+#pragma unroll
+                        for (int d = 0; d < ND; d++) {
+                            const T skl = ((ml >> (c * ND + d)) & 1ull)
+                                              ? (T)__ldg(cd.S + (c * ND + d) * cd.sp_stride + spl) : (T)0;
+                            s = fma(I[c * ND + d] * skl, wv[d], s);
+                        }
+                        Kacc[p][c] += (double)s;
+                    }
+                }
+            }
+        }
+    }
+    __syncwarp();
+}
+
+template <int LA, int LB, int LC, int LD, int ORI>
+__global__ void __launch_bounds__(K_THREADS)
+exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity dm, double maxD, double omega,
+                    double thr, double* __restrict__ mat_K, BoysTabs tabs, unsigned long long* __restrict__ qcount,
+                    double fp32_cut)
+{
+    using S = KColShape<LA, LB, LC, LD, ORI>;
+    constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND;
     constexpr int NAC = NA * NC;
     constexpr int NW = K_THREADS / 32;
-    constexpr int NL = CT::NL, P = CT::P, NXT = CT::NXT, NYT = CT::NYT;
-    // phase-2 units: ori 0 -> cd pairs (accumulate K[a][c(u)]), ori 1 -> ab pairs (K[a(u)][c])
-    constexpr int N2 = ORI == 0 ? NC * ND : NA * NB;
-    constexpr int NACC = ORI == 0 ? NA : NC;
-    constexpr int NPASS = (N2 + NL - 1) / NL;
+    constexpr int NL = S::NL, P = S::P, NXT = S::NXT;
+    constexpr int N2 = S::N2, NACC = S::NACC, NPASS = S::NPASS;
     __shared__ double U[NW][P][NXT][N2];
     __shared__ double red[NW][P][N2][NACC];
-    __shared__ int s_cnt[K_JCHUNK + 1];
+    __shared__ int s_nl[K_JCHUNK], s_n64[K_JCHUNK], s_c64[K_JCHUNK + 1], s_c32[K_JCHUNK + 1];
+    const KChunk ch{s_nl, s_n64, s_c64, s_c32};
 
     const int nout = *out.n;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int grp = lane / NL, lig = lane % NL;
     const bool lane_ok = grp < P;
+    const int gsel = lane_ok ? grp : 0;
     const ColLane ln = make_lane<LA, LB, LC, LD, ORI>(lane_ok ? lig : 0, lane_ok ? grp * NL : lane);
 
     for (int o = blockIdx.x; o < nout; o += gridDim.x) {
@@ -102,121 +204,30 @@ exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd,
 
         for (int jb = a0; jb < a1; jb += K_JCHUNK) {
             const int nj = min(K_JCHUNK, a1 - jb);
-            for (int t = threadIdx.x; t < nj; t += K_THREADS) {
-                const double qij = __ldg(ab.rec_q + jb + t);
-                int lo = c0, hi = c1;
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if (fabs(qij * __ldg(cd.rec_q + mid) * maxD) > thr) lo = mid + 1;
-                    else hi = mid;
-                }
-                s_cnt[t + 1] = lo - c0;
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                s_cnt[0] = 0;
-                for (int t = 1; t <= nj; t++) s_cnt[t] += s_cnt[t - 1];
-            }
-            __syncthreads();
-            const int total = s_cnt[nj];
-            if (qcount && threadIdx.x == 0) atomicAdd(qcount, (unsigned long long)total);
-            const int niter = (total + NW * P - 1) / (NW * P);
-            for (int it = 0; it < niter; it++) {
+            k_chunk_scan(ab, cd, jb, nj, c0, c1, maxD, thr, fp32_cut, ch);
+            const int t64 = s_c64[nj], t32 = s_c32[nj];
+            if (qcount && threadIdx.x == 0) atomicAdd(qcount, (unsigned long long)(t64 + t32));
+            const int n64 = (t64 + NW * P - 1) / (NW * P);
+            for (int it = 0; it < n64; it++) {
                 const int w = it * (NW * P) + warp * P + grp;
-                const bool act = lane_ok && w < total;
+                const bool act = lane_ok && w < t64;
                 const int wq = act ? w : 0;
-                // j of the flattened (j, l) index: last t with s_cnt[t] <= wq
-                int lo = 0, hi = nj;
-                while (hi - lo > 1) {
-                    const int mid = (lo + hi) >> 1;
-                    if (s_cnt[mid] <= wq) lo = mid;
-                    else hi = mid;
-                }
-                const int jr = jb + lo;
-                const int lr = c0 + (wq - s_cnt[lo]);
-                const int spj = __ldg(ab.rec_sp + jr), spl = __ldg(cd.rec_sp + lr);
-                const PairGeo bg = load_geo(ab.geo, ab.sp_stride, spj);
-                const PairGeo kg = load_geo(cd.geo, cd.sp_stride, spl);
-                QV q;
-                double F[L + 1];
-                make_quartet<L>(bg, kg, omega, boys_tab, q, F);
-                double col[NYT];
-                col_vrr<LA, LB, LC, LD, ORI>(q, F, ln, col);
-                // phase 2a: this lane's HRR over the step side, into shared memory
-                if (lane_ok && ln.tidx >= 0) {
-                    double h[N2];
-                    if (ORI == 0) hrr_bra_vector<LC, LD>(q.CDx, q.CDy, q.CDz, col, h);
-                    else hrr_bra_vector<LA, LB>(q.ABx, q.ABy, q.ABz, col, h);
-#pragma unroll
-                    for (int u = 0; u < N2; u++) U[warp][grp][ln.tidx][u] = h[u];
-                }
-                __syncwarp();
-                // phase 2b: fixed units of the other side per lane
-                if (act) {
-                    const int jsh = __ldg(ab.partner + spj), lsh = __ldg(cd.partner + spl);
-                    const uint64_t mj = __ldg(ab.rec_mask + jr), ml = __ldg(cd.rec_mask + lr);
-#pragma unroll
-                    for (int p = 0; p < NPASS; p++) {
-                        const int u = lig + NL * p;
-                        if (u < N2) {
-                            double v[NXT];
-#pragma unroll
-                            for (int x = 0; x < NXT; x++) v[x] = U[warp][grp][x][u];
-                            if (ORI == 0) {
-                                // unit = (c, d): bra HRR, then K[a][c] += sum_b (ab|cd) Sij[ab] Skl[cd] D[b][d]
-                                const int cc = u / ND, dd = u % ND;
-                                double I[NA * NB];
-                                hrr_bra_vector<LA, LB>(q.ABx, q.ABy, q.ABz, v, I);
-                                const double skl = ((ml >> u) & 1ull) ? __ldg(cd.S + u * cd.sp_stride + spl) : 0.0;
-                                const uint32_t lao = __ldg(d_aoinds + lsh + (int64_t)d_count * dd);
-                                double wv[NB];
-#pragma unroll
-                                for (int b = 0; b < NB; b++) {
-                                    const uint32_t jao = __ldg(b_aoinds + jsh + (int64_t)b_count * b);
-                                    wv[b] = skl * __ldg(Dao + (int64_t)jao * naos + lao);
-                                }
-#pragma unroll
-                                for (int a = 0; a < NA; a++) {
-                                    double s = 0.0;
-#pragma unroll
-                                    for (int b = 0; b < NB; b++) {
-                                        const double sij = ((mj >> (a * NB + b)) & 1ull)
-                                                               ? __ldg(ab.S + (a * NB + b) * ab.sp_stride + spj) : 0.0;
-                                        s = fma(I[a * NB + b] * sij, wv[b], s);
-                                    }
-                                    Kacc[p][a] += s;
-                                }
-                                (void)cc;
-                            } else {
-                                // unit = (a, b): ket HRR, then K[a][c] += Sij[ab] sum_d (ab|cd) Skl[cd] D[b][d]
-                                const int aa = u / NB, bb = u % NB;
-                                double I[NC * ND];
-                                hrr_bra_vector<LC, LD>(q.CDx, q.CDy, q.CDz, v, I);
-                                const double sij = ((mj >> u) & 1ull) ? __ldg(ab.S + u * ab.sp_stride + spj) : 0.0;
-                                const uint32_t jao = __ldg(b_aoinds + jsh + (int64_t)b_count * bb);
-                                double wv[ND];
-#pragma unroll
-                                for (int d = 0; d < ND; d++) {
-                                    const uint32_t lao = __ldg(d_aoinds + lsh + (int64_t)d_count * d);
-                                    wv[d] = sij * __ldg(Dao + (int64_t)jao * naos + lao);
-                                }
-#pragma unroll
-                                for (int c = 0; c < NC; c++) {
-                                    double s = 0.0;
-#pragma unroll
-                                    for (int d = 0; d < ND; d++) {
-                                        const double skl = ((ml >> (c * ND + d)) & 1ull)
-                                                               ? __ldg(cd.S + (c * ND + d) * cd.sp_stride + spl) : 0.0;
-                                        s = fma(I[c * ND + d] * skl, wv[d], s);
-                                    }
-                                    Kacc[p][c] += s;
-                                }
-                                (void)aa;
-                            }
-                        }
-                    }
-                }
-                __syncwarp();
+                const int jj = k_find(s_c64, nj, wq);
+                const int jr = jb + jj;
+                const int lr = c0 + (wq - s_c64[jj]);
+                kcol_quartet<LA, LB, LC, LD, ORI, double>(act, jr, act ? lr : c0, ab, cd, dm, omega, tabs, ln,
+                                                          lane_ok, lig, U[warp][gsel], Kacc);
+            }
+            const int n32 = (t32 + NW * P - 1) / (NW * P);
+            for (int it = 0; it < n32; it++) {
+                const int w = it * (NW * P) + warp * P + grp;
+                const bool act = lane_ok && w < t32;
+                const int wq = act ? w : 0;
+                const int jj = k_find(s_c32, nj, wq);
+                const int jr = jb + jj;
+                const int lr = c0 + s_n64[jj] + (wq - s_c32[jj]);
+                kcol_quartet<LA, LB, LC, LD, ORI, float>(act, jr, act ? lr : c0, ab, cd, dm, omega, tabs, ln,
+                                                         lane_ok, lig, U[warp][gsel], Kacc);
             }
             __syncthreads();
         }
@@ -225,7 +236,6 @@ exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd,
         if (lane_ok) {
 #pragma unroll
             for (int p = 0; p < NPASS; p++)
-#pragma unroll
                 if (lig + NL * p < N2)
 #pragma unroll
                     for (int x = 0; x < NACC; x++) red[warp][grp][lig + NL * p][x] = Kacc[p][x];
@@ -250,20 +260,42 @@ exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd,
 }
 
 // ---------------------------------------------------------------- coulomb
+template <int LA, int LB, int LC, int LD, typename T>
+__device__ __forceinline__ void jcol_quartet(bool act, const PairGeo& b, double qb, const JKetPairs& ket, int kt,
+                                             double thr, const BoysTabs& tabs, const ColLane& ln, bool lane_ok,
+                                             double& X)
+{
+    constexpr int L = LA + LB + LC + LD;
+    constexpr int NF = nrange(LC, LD);
+    const PairGeo k = load_geo(ket.geo, ket.stride, kt);
+    QVT<T> q;
+    T F[L + 1];
+    make_quartet_t<L>(b, k, 0.0, tabs.f64, tabs.f32, q, F);
+    T col[NF];
+    col_vrr<LA, LB, LC, LD, 0, T>(q, F, ln, col);
+    if (act && lane_ok && ln.tidx >= 0) {
+        T Dpp[NF];
+        ket_density<LC, LD, T>(ket, kt, qb, thr, k, Dpp);
+        T s = (T)0;
+#pragma unroll
+        for (int f = 0; f < NF; f++) s = fma(col[f], Dpp[f], s);
+        X += (double)s;
+    }
+}
+
 template <int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(J_THREADS)
-coulomb_col_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double thr,
-                   const double* __restrict__ boys_tab, unsigned long long* __restrict__ qcount)
+coulomb_col_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double thr, BoysTabs tabs,
+                   unsigned long long* __restrict__ qcount, double fp32_cut)
 {
     using CT = ColTab<LA, LB, LC, LD, 0>;
-    constexpr int L = LA + LB + LC + LD;
     constexpr int NE = nrange(LA, LB), NF = nrange(LC, LD);
-    constexpr int NAB = ncart(LA) * ncart(LB), NCD = ncart(LC) * ncart(LD);
+    constexpr int NAB = ncart(LA) * ncart(LB);
     constexpr int NW = J_THREADS / 32;
     constexpr int NL = CT::NL, P = CT::P;
     static_assert(CT::NXT == NE && CT::NYT == NF, "column layout");
     __shared__ double red[NW][P][NE];
-    __shared__ int s_ncut;
+    __shared__ int s_ncut, s_n64;
     const int nbra = *bra.n_rec;
     const int nket = *ket.n;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -276,55 +308,27 @@ coulomb_col_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, doub
         const PairGeo b = load_geo(bra.geo, bra.sp_stride, sp);
         const double qb = __ldg(bra.rec_q + r);
         if (threadIdx.x == 0) {
-            int lo = 0, hi = nket;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (qb * __ldg(ket.tmax + mid) * (1.0 + SCREEN_SLACK) > thr) lo = mid + 1;
-                else hi = mid;
-            }
-            s_ncut = lo;
-            int lo2 = 0, hi2 = lo;
-            while (lo2 < hi2) {
-                const int mid = (lo2 + hi2) >> 1;
-                if (qb * __ldg(ket.tmax + mid) > thr) lo2 = mid + 1;
-                else hi2 = mid;
-            }
-            if (qcount) atomicAdd(qcount, (unsigned long long)lo2);
+            int ncut, nexact, n64;
+            ket_prefixes(ket, nket, qb, thr, fp32_cut, ncut, nexact, n64);
+            s_ncut = ncut;
+            s_n64 = n64;
+            if (qcount) atomicAdd(qcount, (unsigned long long)nexact);
         }
         __syncthreads();
-        const int ncut = s_ncut;
+        const int ncut = s_ncut, n64 = s_n64;
         double X = 0.0;
-        const int niter = (ncut + NW * P - 1) / (NW * P);
-        for (int it = 0; it < niter; it++) {
+        const int it64 = (n64 + NW * P - 1) / (NW * P);
+        for (int it = 0; it < it64; it++) {
             const int kt0 = it * (NW * P) + warp * P + grp;
+            const bool act = lane_ok && kt0 < n64;
+            jcol_quartet<LA, LB, LC, LD, double>(act, b, qb, ket, act ? kt0 : 0, thr, tabs, ln, lane_ok, X);
+        }
+        const int n32 = ncut - n64;
+        const int it32 = (n32 + NW * P - 1) / (NW * P);
+        for (int it = 0; it < it32; it++) {
+            const int kt0 = n64 + it * (NW * P) + warp * P + grp;
             const bool act = lane_ok && kt0 < ncut;
-            const int kt = act ? kt0 : 0;
-            const PairGeo k = load_geo(ket.geo, ket.stride, kt);
-            QV q;
-            double F[L + 1];
-            make_quartet<L>(b, k, 0.0, boys_tab, q, F);
-            double col[NF];
-            col_vrr<LA, LB, LC, LD, 0>(q, F, ln, col);
-            if (act && ln.tidx >= 0) {
-                double Dpp[NF];
-                if (qb * __ldg(ket.tmin + kt) > thr * (1.0 + SCREEN_SLACK)) {
-#pragma unroll
-                    for (int f = 0; f < NF; f++) Dpp[f] = __ldg(ket.Dpp + f * ket.stride + kt);
-                } else {
-                    double Dm[NCD];
-#pragma unroll
-                    for (int c = 0; c < NCD; c++) {
-                        const double qk = __ldg(ket.Qc + c * ket.stride + kt);
-                        const double dk = __ldg(ket.Dc + c * ket.stride + kt);
-                        Dm[c] = (fabs(qb * qk * dk) > thr) ? __ldg(ket.Dm + c * ket.stride + kt) : 0.0;
-                    }
-                    hrr_ket_adjoint<LC, LD>(k.Rx, k.Ry, k.Rz, Dm, Dpp);
-                }
-                double s = 0.0;
-#pragma unroll
-                for (int f = 0; f < NF; f++) s = fma(col[f], Dpp[f], s);
-                X += s;
-            }
+            jcol_quartet<LA, LB, LC, LD, float>(act, b, qb, ket, act ? kt0 : 0, thr, tabs, ln, lane_ok, X);
         }
         if (lane_ok && ln.tidx >= 0) red[warp][grp][ln.tidx] = X;
         __syncthreads();
@@ -338,7 +342,7 @@ coulomb_col_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, doub
                 Xs[e] = s;
             }
             double J[NAB];
-            hrr_bra_vector<LA, LB>(b.Rx, b.Ry, b.Rz, Xs, J);
+            hrr_bra_vector<LA, LB, double>(b.Rx, b.Ry, b.Rz, Xs, J);
             const uint64_t mask = __ldg(bra.rec_mask + r);
 #pragma unroll
             for (int c = 0; c < NAB; c++) {

@@ -63,13 +63,51 @@ __device__ __forceinline__ void boys_f64(double T, const double* __restrict__ ta
     }
 }
 
+// FP32 variant for the mixed-precision path: the Boys argument T arrives in
+// FP64; F_L from a float copy of the same table (4 Taylor terms: truncation
+// < 2e-8 relative, below float rounding), recursions in float.
+constexpr int BOYS_NT32 = 4;
+
+template <int L>
+__device__ __forceinline__ void boys_f32(double Td, const float* __restrict__ tab, float* F)
+{
+    if (Td < BOYS_TMAX) {
+        const int k = __double2int_rn(Td * BOYS_INV_H);
+        const float md = (float)((double)k * BOYS_H - Td);
+        const float T = (float)Td;
+        const float* row = tab + k * BOYS_NCOL + L;
+        float acc = __ldg(row + BOYS_NT32 - 1);
+#pragma unroll
+        for (int j = BOYS_NT32 - 1; j >= 1; j--) acc = fmaf(acc, md * (1.0f / j), __ldg(row + j - 1));
+        F[L] = acc;
+        if (L > 0) {
+            const float ex = __expf(-T);
+            const float t2 = 2.0f * T;
+#pragma unroll
+            for (int m = L - 1; m >= 0; m--) F[m] = fmaf(t2, F[m + 1], ex) * (1.0f / (2.0f * m + 1.0f));
+        }
+    } else {
+        const float T = (float)Td;
+        const float inv_t = 1.0f / T;
+        F[0] = (float)SQRT_PI_4 * sqrtf(inv_t);
+        if (L > 0) {
+            const float ex = __expf(-T);
+            const float h = 0.5f * inv_t;
+#pragma unroll
+            for (int m = 0; m < L; m++) F[m + 1] = fmaf((2.0f * m + 1.0f), F[m], -ex) * h;
+        }
+    }
+}
+
 // ---------------------------------------------------------------- quartet
-struct QV {
-    double PAx, PAy, PAz, WPx, WPy, WPz;
-    double QCx, QCy, QCz, WQx, WQy, WQz;
-    double ABx, ABy, ABz, CDx, CDy, CDz;
-    double inv2z, inv2e, inv2ze, rz, re;
+template <typename T>
+struct QVT {
+    T PAx, PAy, PAz, WPx, WPy, WPz;
+    T QCx, QCy, QCz, WQx, WQy, WQz;
+    T ABx, ABy, ABz, CDx, CDy, CDz;
+    T inv2z, inv2e, inv2ze, rz, re;
 };
+using QV = QVT<double>;
 
 // Primitive-pair geometry records (one per primitive shell pair), SoA in HBM.
 // Bra: zeta, 0.5/zeta, P[3], PA = P - A [3], AB = A - B [3].
@@ -131,14 +169,60 @@ __device__ __forceinline__ void make_quartet(const PairGeo& b, const PairGeo& k,
     }
 }
 
-template <int LA, int LB, int LC, int LD>
-__device__ __forceinline__ void eri_full(const QV& q, const double* F, double* out);
-template <int LA, int LB, int LC, int LD>
-__device__ __forceinline__ void j_contract(const QV& q, const double* F, const double* Dpp, double* X);
-template <int LC, int LD>
-__device__ __forceinline__ void hrr_ket_adjoint(double CDx, double CDy, double CDz, const double* Dm, double* Dpp);
-template <int LA, int LB>
-__device__ __forceinline__ void hrr_bra_vector(double ABx, double ABy, double ABz, const double* X, double* J);
+// Mixed-precision variant of make_quartet: every quartet scalar and the Boys
+// argument are formed in FP64 and rounded to float; F_m in float.
+template <int L>
+__device__ __forceinline__ void make_quartet_f32(const PairGeo& b, const PairGeo& k, double omega,
+                                                 const float* __restrict__ boys_tab32, QVT<float>& q, float* F)
+{
+    const double inv = 1.0 / (b.z + k.z);
+    const double rho = b.z * k.z * inv;
+    const double PQx = k.Px - b.Px, PQy = k.Py - b.Py, PQz = k.Pz - b.Pz;
+    const double rz = k.z * inv, re = b.z * inv;
+    q.PAx = (float)b.Ax; q.PAy = (float)b.Ay; q.PAz = (float)b.Az;
+    q.ABx = (float)b.Rx; q.ABy = (float)b.Ry; q.ABz = (float)b.Rz;
+    q.QCx = (float)k.Ax; q.QCy = (float)k.Ay; q.QCz = (float)k.Az;
+    q.CDx = (float)k.Rx; q.CDy = (float)k.Ry; q.CDz = (float)k.Rz;
+    q.WPx = (float)(rz * PQx); q.WPy = (float)(rz * PQy); q.WPz = (float)(rz * PQz);
+    q.WQx = (float)(-re * PQx); q.WQy = (float)(-re * PQy); q.WQz = (float)(-re * PQz);
+    q.inv2z = (float)b.i2z; q.inv2e = (float)k.i2z; q.inv2ze = (float)(0.5 * inv);
+    q.rz = (float)rz; q.re = (float)re;
+    const double r2 = fma(PQx, PQx, fma(PQy, PQy, PQz * PQz));
+    double d2 = 1.0;
+    if (omega != 0.0) d2 = omega * omega / (rho + omega * omega);
+    const double rd = rho * d2;
+    boys_f32<L>(rd * r2, boys_tab32, F);
+    const float lam = (float)(2.0 * sqrt(rd * INV_PI_D));
+    float s = lam;
+    const float d2f = (float)d2;
+#pragma unroll
+    for (int m = 0; m <= L; m++) { F[m] *= s; s *= d2f; }
+}
+
+// Precision-generic quartet set-up (overloaded on the output type).
+template <int L>
+__device__ __forceinline__ void make_quartet_t(const PairGeo& b, const PairGeo& k, double omega,
+                                               const double* __restrict__ tab64, const float* __restrict__ tab32,
+                                               QVT<double>& q, double* F)
+{
+    make_quartet<L>(b, k, omega, tab64, q, F);
+}
+template <int L>
+__device__ __forceinline__ void make_quartet_t(const PairGeo& b, const PairGeo& k, double omega,
+                                               const double* __restrict__ tab64, const float* __restrict__ tab32,
+                                               QVT<float>& q, float* F)
+{
+    make_quartet_f32<L>(b, k, omega, tab32, q, F);
+}
+
+template <int LA, int LB, int LC, int LD, typename T>
+__device__ __forceinline__ void eri_full(const QVT<T>& q, const T* F, T* out);
+template <int LA, int LB, int LC, int LD, typename T>
+__device__ __forceinline__ void j_contract(const QVT<T>& q, const T* F, const T* Dpp, T* X);
+template <int LC, int LD, typename T>
+__device__ __forceinline__ void hrr_ket_adjoint(T CDx, T CDy, T CDz, const T* Dm, T* Dpp);
+template <int LA, int LB, typename T>
+__device__ __forceinline__ void hrr_bra_vector(T ABx, T ABy, T ABz, const T* X, T* J);
 
 __host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 // number of Cartesian components with |e| in [l0, l0 + l1]

@@ -64,6 +64,14 @@ class Arena {
 // (table upload); call vlxb_init() before any stream capture.
 const double* boys_table_device();
 
+// Float copy of the same table for the mixed-precision path.
+const float* boys_table32_device();
+
+// Quartets whose screening bound is below this value are evaluated in FP32
+// (0 = plain FP64, the default of the drop-in entry points).
+double fp32_cut_get();
+int fp32_cut_set(double cut);
+
 // Per-device counters of screened-in primitive shell quartets processed by
 // the J ([0]) and K ([1]) kernels (device memory, allocated with the table).
 unsigned long long* quartet_counters_device();

@@ -146,7 +146,14 @@ def header():
          "   choice only changes speed.  Set by the autotuner.  No reference",
          "   counterpart. */",
          "int vlxb_setSchedule(int kind, int la, int lb, int lc, int ld, int variant);",
-         "int vlxb_getSchedule(int kind, int la, int lb, int lc, int ld);", ""]
+         "int vlxb_getSchedule(int kind, int la, int lb, int lc, int ld);", "",
+         "/* Mixed precision: shell quartets whose screening bound (|Q_ij| max|Q_kl D_kl|",
+         "   for J, |Q_ij Q_kl max_D| for K) is below `cutoff` are evaluated in FP32",
+         "   (Boys argument in FP64), everything else and all accumulation in FP64.",
+         "   0 (the default) = plain FP64, the drop-in behaviour.  Process-wide.",
+         "   No reference counterpart. */",
+         "int vlxb_setFp32Cutoff(double cutoff);",
+         "double vlxb_getFp32Cutoff(void);", ""]
     L.append("/* ---- Coulomb: replace computeCoulombFock<ABCD> of gen_coulomb.py:74-93 ---- */")
     for cls in j_classes():
         L.append(f"/* replaces computeCoulombFock{cls.upper()} (gen_coulomb.py:74-93; class list gen_coulomb.py:47-56) */")

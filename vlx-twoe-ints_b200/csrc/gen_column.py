@@ -272,12 +272,14 @@ def _yname(y):
     return f"{y[0]}{y[1]}{y[2]}"
 
 
-def emit_cuda(plan: ColumnPlan):
+def emit_cuda(plan: ColumnPlan, T: str = "double", with_tables: bool = True):
     """Device function col_vrr<LA,LB,LC,LD,ORI>(q, F, ln, out): out[t] = [x|y_t]^0 for
     the lane's component x and the step-side targets y_t (plan.ytargets order).
     Also the lane table col_tab<...> (plan.NL rows of 20 int8)."""
     la, lb, lc, ld = plan.cls
     ori = plan.ori
+    TT = T
+    lit = "f" if T == "float" else ""
     T = f"{la}, {lb}, {lc}, {ld}, {ori}"
     if ori == 0:
         PX, WX, i2X, rX = ["q.PAx", "q.PAy", "q.PAz"], ["q.WPx", "q.WPy", "q.WPz"], "q.inv2z", "q.rz"
@@ -287,40 +289,41 @@ def emit_cuda(plan: ColumnPlan):
         PY, WY, i2Y, rY = ["q.PAx", "q.PAy", "q.PAz"], ["q.WPx", "q.WPy", "q.WPz"], "q.inv2z", "q.rz"
     L = []
     rows = []
-    for k in range(plan.NL):
+    for k in range(plan.NL if with_tables else 0):
         st = plan.lane_static(k)
         row = list(st["x"]) + st["src"] + st["jdir"] + st["cdir"] + st["ck"] + [st["level"], st["tidx"], 0]
         rows.append("{" + ", ".join(str(v) for v in row) + "}")
-    L.append(f"template <> struct ColTab<{T}> {{")
-    L.append(f"    static constexpr int NL = {plan.NL}, P = {plan.P}, NXT = {len(plan.xtargets)}, "
-             f"NYT = {len(plan.ytargets)}, LAM = {plan.lam};")
-    L.append(f"    static constexpr bool K_FITS = {'true' if k_smem_bytes(plan) <= 46 * 1024 else 'false'};"
-             f"  // exchange kernel shared memory: {k_smem_bytes(plan)} bytes")
-    L.append("};")
-    L.append(f"__device__ const int8_t col_tab_{plan.name()}[{plan.NL}][20] = {{" + ", ".join(rows) + "};")
-    L.append(f"template <> __device__ __forceinline__ const int8_t* col_tab_ptr<{T}>() "
-             f"{{ return &col_tab_{plan.name()}[0][0]; }}")
-    L.append("")
-    L.append(f"template <> __device__ __forceinline__ void col_vrr<{T}>(const QV& q, const double* F, "
-             "const ColLane& ln, double* out)")
+    if with_tables:
+        L.append(f"template <> struct ColTab<{T}> {{")
+        L.append(f"    static constexpr int NL = {plan.NL}, P = {plan.P}, NXT = {len(plan.xtargets)}, "
+                 f"NYT = {len(plan.ytargets)}, LAM = {plan.lam};")
+        L.append(f"    static constexpr bool K_FITS = {'true' if k_smem_bytes(plan) <= 46 * 1024 else 'false'};"
+                 f"  // exchange kernel shared memory: {k_smem_bytes(plan)} bytes")
+        L.append("};")
+        L.append(f"__device__ const int8_t col_tab_{plan.name()}[{plan.NL}][20] = {{" + ", ".join(rows) + "};")
+        L.append(f"template <> __device__ __forceinline__ const int8_t* col_tab_ptr<{T}>() "
+                 f"{{ return &col_tab_{plan.name()}[0][0]; }}")
+        L.append("")
+    L.append(f"template <> __device__ __forceinline__ void col_vrr<{T}, {TT}>(const QVT<{TT}>& q, const {TT}* F, "
+             f"const ColLane& ln, {TT}* out)")
     L.append("{")
-    L.append(f"    const double cpl = q.inv2ze;")
-    L.append("    const double cp0 = ln.xi[0] * cpl, cp1 = ln.xi[1] * cpl, cp2 = ln.xi[2] * cpl;")
+    L.append(f"    const {TT} cpl = q.inv2ze;")
+    L.append(f"    const {TT} cp0 = ({TT})ln.xi[0] * cpl, cp1 = ({TT})ln.xi[1] * cpl, cp2 = ({TT})ln.xi[2] * cpl;")
     L.append("    (void)cp0; (void)cp1; (void)cp2;")
     # chain
     M0 = plan.chain_m[0]
     for m in range(M0 + 2):
-        L.append(f"    double b{m} = {'F[' + str(m) + ']' if m <= M0 else '0.0'}, p{m} = 0.0;")
+        L.append(f"    {TT} b{m} = {'F[' + str(m) + ']' if m <= M0 else '0'}, p{m} = 0;")
     for s in range(1, plan.chain_len + 1):
         M = plan.chain_m[s]
         L.append("    {")
         L.append(f"        const int d = ln.cdir[{s - 1}];")
         L.append("        const bool act = d >= 0;")
-        L.append(f"        const double Pd = d == 0 ? {PX[0]} : (d == 1 ? {PX[1]} : {PX[2]});")
-        L.append(f"        const double Wd = d == 0 ? {WX[0]} : (d == 1 ? {WX[1]} : {WX[2]});")
-        L.append(f"        const double kd = ln.ck[{s - 1}] * {i2X};")
+        L.append(f"        const {TT} Pd = d == 0 ? {PX[0]} : (d == 1 ? {PX[1]} : {PX[2]});")
+        L.append(f"        const {TT} Wd = d == 0 ? {WX[0]} : (d == 1 ? {WX[1]} : {WX[2]});")
+        L.append(f"        const {TT} kd = ({TT})ln.ck[{s - 1}] * {i2X};")
         for m in range(M + 1):
-            L.append(f"        const double n{m} = fma(kd, fma(-{rX}, p{m + 1}, p{m}), fma(Pd, b{m}, Wd * b{m + 1}));")
+            L.append(f"        const {TT} n{m} = fma(kd, fma(-{rX}, p{m + 1}, p{m}), fma(Pd, b{m}, Wd * b{m + 1}));")
         for m in range(M + 1):
             L.append(f"        p{m} = act ? b{m} : p{m}; b{m} = act ? n{m} : b{m};")
         L.append("    }")
@@ -337,39 +340,39 @@ def emit_cuda(plan: ColumnPlan):
         e = f"fma({WY[i]}, {tname[(g1, m + 1)]}, {PY[i]} * {tname[(g1, m)]})"
         if g1[i] > 0:
             g2 = sub1(g1, i)
-            e = f"fma({g1[i]}.0 * {i2Y}, fma(-{rY}, {tname[(g2, m + 1)]}, {tname[(g2, m)]}), {e})"
+            e = f"fma({g1[i]}.0{lit} * {i2Y}, fma(-{rY}, {tname[(g2, m + 1)]}, {tname[(g2, m)]}), {e})"
         nm = f"t{_yname(g)}_{m}"
-        L.append(f"    const double {nm} = {e};")
+        L.append(f"    const {TT} {nm} = {e};")
         tname[(g, m)] = nm
     if plan.derive:
         L.append("    // level-lam lanes: coupling partners of level lam-1 derived from the tower")
         for i in range(3):
             L.append(f"    const int jd{i} = ln.jdir[{i}];")
-            L.append(f"    const double jP{i} = jd{i} == 0 ? {PX[0]} : (jd{i} == 1 ? {PX[1]} : {PX[2]});")
-            L.append(f"    const double jW{i} = jd{i} == 0 ? {WX[0]} : (jd{i} == 1 ? {WX[1]} : {WX[2]});")
+            L.append(f"    const {TT} jP{i} = jd{i} == 0 ? {PX[0]} : (jd{i} == 1 ? {PX[1]} : {PX[2]});")
+            L.append(f"    const {TT} jW{i} = jd{i} == 0 ? {WX[0]} : (jd{i} == 1 ? {WX[1]} : {WX[2]});")
     # steps
     for (y, m) in plan.step_nodes:
         i = first_nz(y)
         y1 = sub1(y, i)
         nm = f"c{_yname(y)}_{m}"
-        L.append(f"    const double sh_{nm} = __shfl_sync(0xffffffffu, {cname[(y1, m + 1)]}, ln.src[{i}]);")
+        L.append(f"    const {TT} sh_{nm} = __shfl_sync(0xffffffffu, {cname[(y1, m + 1)]}, ln.src[{i}]);")
         cp = f"sh_{nm}"
         if plan.need_derived[(y, m)]:
             g = y1
-            gj = f"(jd{i} == 0 ? {g[0]}.0 : (jd{i} == 1 ? {g[1]}.0 : {g[2]}.0))"
+            gj = f"(jd{i} == 0 ? {g[0]}.0{lit} : (jd{i} == 1 ? {g[1]}.0{lit} : {g[2]}.0{lit}))"
             tl = []
             for j in range(3):
-                tl.append(tname[(sub1(g, j), m + 2)] if g[j] > 0 else "0.0")
+                tl.append(tname[(sub1(g, j), m + 2)] if g[j] > 0 else f"0.0{lit}")
             tsel = f"(jd{i} == 0 ? {tl[0]} : (jd{i} == 1 ? {tl[1]} : {tl[2]}))"
             der = (f"fma({gj} * cpl, {tsel}, fma(jP{i}, {tname[(g, m + 1)]}, jW{i} * {tname[(g, m + 2)]}))")
-            L.append(f"    const double cv_{nm} = ln.lamlane ? {der} : sh_{nm};")
+            L.append(f"    const {TT} cv_{nm} = ln.lamlane ? {der} : sh_{nm};")
             cp = f"cv_{nm}"
         e = f"fma({WY[i]}, {cname[(y1, m + 1)]}, {PY[i]} * {cname[(y1, m)]})"
         if y1[i] > 0:
             y2 = sub1(y1, i)
-            e = f"fma({y1[i]}.0 * {i2Y}, fma(-{rY}, {cname[(y2, m + 1)]}, {cname[(y2, m)]}), {e})"
+            e = f"fma({y1[i]}.0{lit} * {i2Y}, fma(-{rY}, {cname[(y2, m + 1)]}, {cname[(y2, m)]}), {e})"
         e = f"fma(cp{i}, {cp}, {e})"
-        L.append(f"    const double {nm} = {e};")
+        L.append(f"    const {TT} {nm} = {e};")
         cname[(y, m)] = nm
     for t, y in enumerate(plan.ytargets):
         L.append(f"    out[{t}] = {cname[(y, 0)]};")
@@ -427,7 +430,9 @@ def main(outdir):
         name = "".join("spd"[l] for l in cls)
         parts = ["// Generated by gen_column.py -- do not edit.", "#pragma once", "namespace vlxb {", ""]
         for ori in (0, 1):
-            parts.append(emit_cuda(ColumnPlan(*cls, ori)))
+            parts.append(emit_cuda(ColumnPlan(*cls, ori), "double", True))
+            parts.append("")
+            parts.append(emit_cuda(ColumnPlan(*cls, ori), "float", False))
             parts.append("")
         parts.append("}  // namespace vlxb")
         text = "\n".join(parts) + "\n"

@@ -189,18 +189,19 @@ class HRR:
         return [n for n in self.order if sum(n[1]) == 0]
 
 
-def q_prologue(la, lb, lc, ld):
+def q_prologue(la, lb, lc, ld, T="double"):
+    lit = "f" if T == "float" else ""
     lines = []
     for k in range(1, la + lb + 1):
-        lines.append(f"    const double c2z_{k} = {k}.0 * q.inv2z; (void)c2z_{k};")
+        lines.append(f"    const {T} c2z_{k} = {k}.0{lit} * q.inv2z; (void)c2z_{k};")
     for k in range(1, lc + ld + 1):
-        lines.append(f"    const double c2e_{k} = {k}.0 * q.inv2e; (void)c2e_{k};")
+        lines.append(f"    const {T} c2e_{k} = {k}.0{lit} * q.inv2e; (void)c2e_{k};")
     for k in range(1, la + lb + 1):
-        lines.append(f"    const double c2ze_{k} = {k}.0 * q.inv2ze; (void)c2ze_{k};")
+        lines.append(f"    const {T} c2ze_{k} = {k}.0{lit} * q.inv2ze; (void)c2ze_{k};")
     return lines
 
 
-def gen_vrr_block(la, lb, lc, ld, fl, sink):
+def gen_vrr_block(la, lb, lc, ld, fl, sink, T="double"):
     """Straight-line VRR; sink(node, varname) -> extra lines after a target."""
     E = erange(la, la + lb)
     Fs = erange(lc, lc + ld)
@@ -216,28 +217,28 @@ def gen_vrr_block(la, lb, lc, ld, fl, sink):
     for idx, node in enumerate(v.order):
         nm = f"v{idx}"
         names[node] = nm
-        lines.append(f"    const double {nm} = {v.expr(node, name, fl)};")
+        lines.append(f"    const {T} {nm} = {v.expr(node, name, fl)};")
         if node in tset:
             lines += sink(node, nm)
     return lines, E, Fs
 
 
-def gen_eri_full(la, lb, lc, ld):
+def gen_eri_full(la, lb, lc, ld, T="double"):
     fl = Flops()
     E = erange(la, la + lb)
     Fs = erange(lc, lc + ld)
     eidx = {e: i for i, e in enumerate(E)}
     fidx = {f: i for i, f in enumerate(Fs)}
-    lines = [f"template <> __device__ __forceinline__ void eri_full<{la}, {lb}, {lc}, {ld}>"
-             "(const QV& q, const double* F, double* out)", "{"]
-    lines += q_prologue(la, lb, lc, ld)
+    lines = [f"template <> __device__ __forceinline__ void eri_full<{la}, {lb}, {lc}, {ld}, {T}>"
+             f"(const QVT<{T}>& q, const {T}* F, {T}* out)", "{"]
+    lines += q_prologue(la, lb, lc, ld, T)
     tnames = {}
 
     def sink(node, nm):
         tnames[(node[0], node[1])] = nm
         return []
 
-    vl, _, _ = gen_vrr_block(la, lb, lc, ld, fl, sink)
+    vl, _, _ = gen_vrr_block(la, lb, lc, ld, fl, sink, T)
     lines += vl
     # ket HRR per e
     hk = HRR(lc, ld)
@@ -252,7 +253,7 @@ def gen_eri_full(la, lb, lc, ld):
             a1 = ket_names[(e, add1(x, i), sub1(y, i))]
             a2 = ket_names[(e, x, sub1(y, i))]
             nm = f"k{eidx[e]}_{hk.index[node]}"
-            lines.append(f"    const double {nm} = fma(q.CD{'xyz'[i]}, {a2}, {a1});")
+            lines.append(f"    const {T} {nm} = fma(q.CD{'xyz'[i]}, {a2}, {a1});")
             fl.fma += 1
             ket_names[(e, x, y)] = nm
     # bra HRR per (c, d)
@@ -272,7 +273,7 @@ def gen_eri_full(la, lb, lc, ld):
                 a1 = bra_names[(add1(x, i), sub1(y, i))]
                 a2 = bra_names[(x, sub1(y, i))]
                 nm = f"b{ic}_{id_}_{hb.index[node]}"
-                lines.append(f"    const double {nm} = fma(q.AB{'xyz'[i]}, {a2}, {a1});")
+                lines.append(f"    const {T} {nm} = fma(q.AB{'xyz'[i]}, {a2}, {a1});")
                 fl.fma += 1
                 bra_names[node] = nm
             for ia, a in enumerate(Aa):
@@ -283,40 +284,40 @@ def gen_eri_full(la, lb, lc, ld):
     return lines, fl
 
 
-def gen_j_contract(la, lb, lc, ld):
+def gen_j_contract(la, lb, lc, ld, T="double"):
     fl = Flops()
     E = erange(la, la + lb)
     Fs = erange(lc, lc + ld)
     eidx = {e: i for i, e in enumerate(E)}
     fidx = {f: i for i, f in enumerate(Fs)}
-    lines = [f"template <> __device__ __forceinline__ void j_contract<{la}, {lb}, {lc}, {ld}>"
-             "(const QV& q, const double* F, const double* Dpp, double* X)", "{"]
-    lines += q_prologue(la, lb, lc, ld)
+    lines = [f"template <> __device__ __forceinline__ void j_contract<{la}, {lb}, {lc}, {ld}, {T}>"
+             f"(const QVT<{T}>& q, const {T}* F, const {T}* Dpp, {T}* X)", "{"]
+    lines += q_prologue(la, lb, lc, ld, T)
 
     def sink(node, nm):
         fl.fma += 1
         return [f"    X[{eidx[node[0]]}] = fma({nm}, Dpp[{fidx[node[1]]}], X[{eidx[node[0]]}]);"]
 
-    vl, _, _ = gen_vrr_block(la, lb, lc, ld, fl, sink)
+    vl, _, _ = gen_vrr_block(la, lb, lc, ld, fl, sink, T)
     lines += vl
     lines.append("}")
     return lines, fl
 
 
-def gen_hrr_ket_adjoint(lc, ld):
+def gen_hrr_ket_adjoint(lc, ld, T="double"):
     """Dpp_f (f over erange(lc, lc+ld)) = sum_{c,d} H(cd <- f) Dm[c*nd+d]."""
     hk = HRR(lc, ld)
     Fs = erange(lc, lc + ld)
     fidx = {f: i for i, f in enumerate(Fs)}
     Cc, Dd = comps(lc), comps(ld)
     nd = len(Dd)
-    lines = [f"template <> __device__ __forceinline__ void hrr_ket_adjoint<{lc}, {ld}>"
-             "(double CDx, double CDy, double CDz, const double* Dm, double* Dpp)", "{",
-             "    const double CDv[3] = {CDx, CDy, CDz}; (void)CDv;"]
+    lines = [f"template <> __device__ __forceinline__ void hrr_ket_adjoint<{lc}, {ld}, {T}>"
+             f"({T} CDx, {T} CDy, {T} CDz, const {T}* Dm, {T}* Dpp)", "{",
+             f"    const {T} CDv[3] = {{CDx, CDy, CDz}}; (void)CDv;"]
     # adjoint accumulators per node
     adj = {n: f"a{hk.index[n]}" for n in hk.order}
     for n in hk.order:
-        lines.append(f"    double {adj[n]} = 0.0;")
+        lines.append(f"    {T} {adj[n]} = 0;")
     for ic, c in enumerate(Cc):
         for id_, d in enumerate(Dd):
             lines.append(f"    {adj[(c, d)]} += Dm[{ic * nd + id_}];")
@@ -335,16 +336,16 @@ def gen_hrr_ket_adjoint(lc, ld):
     return lines
 
 
-def gen_hrr_bra_vector(la, lb):
+def gen_hrr_bra_vector(la, lb, T="double"):
     """J[a*nb+b] = sum_e H(ab <- e) X_e, e over erange(la, la+lb)."""
     hb = HRR(la, lb)
     E = erange(la, la + lb)
     eidx = {e: i for i, e in enumerate(E)}
     Aa, Bb = comps(la), comps(lb)
     nb = len(Bb)
-    lines = [f"template <> __device__ __forceinline__ void hrr_bra_vector<{la}, {lb}>"
-             "(double ABx, double ABy, double ABz, const double* X, double* J)", "{",
-             "    const double ABv[3] = {ABx, ABy, ABz}; (void)ABv;"]
+    lines = [f"template <> __device__ __forceinline__ void hrr_bra_vector<{la}, {lb}, {T}>"
+             f"({T} ABx, {T} ABy, {T} ABz, const {T}* X, {T}* J)", "{",
+             f"    const {T} ABv[3] = {{ABx, ABy, ABz}}; (void)ABv;"]
     names = {}
     for n in hb.order:
         x, y = n
@@ -353,7 +354,7 @@ def gen_hrr_bra_vector(la, lb):
             continue
         i = first_nz(y)
         nm = f"h{hb.index[n]}"
-        lines.append(f"    const double {nm} = fma(ABv[{i}], {names[(x, sub1(y, i))]}, "
+        lines.append(f"    const {T} {nm} = fma(ABv[{i}], {names[(x, sub1(y, i))]}, "
                      f"{names[(add1(x, i), sub1(y, i))]});")
         names[n] = nm
     for ia, a in enumerate(Aa):
@@ -383,17 +384,21 @@ def main(outdir):
         name = LNAME[la] + LNAME[lb] + LNAME[lc] + LNAME[ld]
         l1, f1 = gen_eri_full(la, lb, lc, ld)
         l2, f2 = gen_j_contract(la, lb, lc, ld)
+        l3, _ = gen_eri_full(la, lb, lc, ld, "float")
+        l4, _ = gen_j_contract(la, lb, lc, ld, "float")
         write_if_changed(os.path.join(outdir, f"q_{name}.cuh"),
                          "\n".join(["// Generated by gen_quartets.py -- do not edit.", "#pragma once",
-                                    "namespace vlxb {", ""] + l1 + [""] + l2 + ["", "}  // namespace vlxb", ""]))
+                                    "namespace vlxb {", ""] + l1 + [""] + l2 + [""] + l3 + [""] + l4
+                                   + ["", "}  // namespace vlxb", ""]))
         flops[name] = {"vrr_hrr_full": f1.total(), "j_contract": f2.total(),
                        "n_vrr": len(VRR([(e, f, 0) for e in erange(la, la + lb)
                                          for f in erange(lc, lc + ld)]).order)}
     pairs = []
     for lc in range(3):
         for ld in range(3):
-            pairs += gen_hrr_ket_adjoint(lc, ld) + [""]
-            pairs += gen_hrr_bra_vector(lc, ld) + [""]
+            for T in ("double", "float"):
+                pairs += gen_hrr_ket_adjoint(lc, ld, T) + [""]
+                pairs += gen_hrr_bra_vector(lc, ld, T) + [""]
     write_if_changed(os.path.join(outdir, "hrr_pairs.cuh"),
                      "\n".join(["// Generated by gen_quartets.py -- do not edit.", "#pragma once",
                                 "namespace vlxb {", ""] + pairs + ["}  // namespace vlxb", ""]))

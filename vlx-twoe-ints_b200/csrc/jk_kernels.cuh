@@ -16,7 +16,15 @@
 // block; its threads stride over the flattened list of (j, l) partner pairs
 // that pass |Q_ij Q_kl max_D| > thr, each accumulating K_ac partials, then
 // reduce in a fixed order and write mat_K[ik] += K_ik.
+//
+// Mixed precision (fp32_cut > 0): quartets whose screening bound
+// (|Q_ij| max|Q_kl D_kl| for J, |Q_ij Q_kl max_D| for K) is below fp32_cut run
+// the same generated code in FP32 (Boys argument formed in FP64); each
+// quartet's result is added to FP64 accumulators.  The sorted lists make the
+// FP64 quartets a prefix and the FP32 ones the segment after it.
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace vlxb {
@@ -52,17 +60,102 @@ struct JKetPairs {
     const int* n;
 };
 
-template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(J_THREADS)
-coulomb_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double thr,
-               const double* __restrict__ boys_tab, unsigned long long* __restrict__ qcount)
+struct BoysTabs {
+    const double* f64;
+    const float* f32;
+};
+
+// Ket density of one quartet as T: the stored D'' when every component passes
+// the screen, else the exact per-component screen (same product order as the
+// reference: fabs(Q_ij * Q_kl * D_kl) <= thr -> skip) through the transposed
+// ket HRR.
+template <int LC, int LD, typename T>
+__device__ __forceinline__ void ket_density(const JKetPairs& ket, int kt, double qb, double thr, const PairGeo& k,
+                                            T* Dpp)
+{
+    constexpr int NCD = ncart(LC) * ncart(LD), NF = nrange(LC, LD);
+    if (qb * __ldg(ket.tmin + kt) > thr * (1.0 + SCREEN_SLACK)) {
+#pragma unroll
+        for (int f = 0; f < NF; f++) Dpp[f] = (T)__ldg(ket.Dpp + f * ket.stride + kt);
+    } else {
+        T Dm[NCD];
+#pragma unroll
+        for (int c = 0; c < NCD; c++) {
+            const double qk = __ldg(ket.Qc + c * ket.stride + kt);
+            const double dk = __ldg(ket.Dc + c * ket.stride + kt);
+            Dm[c] = (fabs(qb * qk * dk) > thr) ? (T)__ldg(ket.Dm + c * ket.stride + kt) : (T)0;
+        }
+        hrr_ket_adjoint<LC, LD, T>((T)k.Rx, (T)k.Ry, (T)k.Rz, Dm, Dpp);
+    }
+}
+
+template <int LA, int LB, int LC, int LD, typename T>
+__device__ __forceinline__ void j_quartet(const PairGeo& b, double qb, const JKetPairs& ket, int kt, double thr,
+                                          const BoysTabs& tabs, double* X)
 {
     constexpr int L = LA + LB + LC + LD;
     constexpr int NE = nrange(LA, LB), NF = nrange(LC, LD);
-    constexpr int NAB = ncart(LA) * ncart(LB), NCD = ncart(LC) * ncart(LD);
+    const PairGeo k = load_geo(ket.geo, ket.stride, kt);
+    QVT<T> q;
+    T F[L + 1];
+    make_quartet_t<L>(b, k, 0.0, tabs.f64, tabs.f32, q, F);
+    T Dpp[NF];
+    ket_density<LC, LD, T>(ket, kt, qb, thr, k, Dpp);
+    if constexpr (std::is_same<T, double>::value) {
+        j_contract<LA, LB, LC, LD, double>(q, F, Dpp, X);
+    } else {
+        T Xq[NE];
+#pragma unroll
+        for (int e = 0; e < NE; e++) Xq[e] = (T)0;
+        j_contract<LA, LB, LC, LD, T>(q, F, Dpp, Xq);
+#pragma unroll
+        for (int e = 0; e < NE; e++) X[e] += (double)Xq[e];
+    }
+}
+
+// Prefix lengths of the descending ket bound list for one bra: ncut (slack
+// included: candidates), nexact (screened-in quartets, for the counters),
+// n64 (bound >= fp32_cut: evaluated in FP64; all of ncut when fp32_cut <= 0).
+__device__ __forceinline__ void ket_prefixes(const JKetPairs& ket, int nket, double qb, double thr,
+                                             double fp32_cut, int& ncut, int& nexact, int& n64)
+{
+    int lo = 0, hi = nket;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (qb * __ldg(ket.tmax + mid) * (1.0 + SCREEN_SLACK) > thr) lo = mid + 1;
+        else hi = mid;
+    }
+    ncut = lo;
+    int lo2 = 0, hi2 = lo;
+    while (lo2 < hi2) {
+        const int mid = (lo2 + hi2) >> 1;
+        if (qb * __ldg(ket.tmax + mid) > thr) lo2 = mid + 1;
+        else hi2 = mid;
+    }
+    nexact = lo2;
+    if (fp32_cut <= 0.0) {
+        n64 = ncut;
+    } else {
+        int lo3 = 0, hi3 = ncut;
+        while (lo3 < hi3) {
+            const int mid = (lo3 + hi3) >> 1;
+            if (qb * __ldg(ket.tmax + mid) >= fp32_cut) lo3 = mid + 1;
+            else hi3 = mid;
+        }
+        n64 = lo3;
+    }
+}
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(J_THREADS)
+coulomb_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double thr, BoysTabs tabs,
+               unsigned long long* __restrict__ qcount, double fp32_cut)
+{
+    constexpr int NE = nrange(LA, LB);
+    constexpr int NAB = ncart(LA) * ncart(LB);
     constexpr int NW = J_THREADS / 32;
     __shared__ double red[NW][NE];
-    __shared__ int s_ncut;
+    __shared__ int s_ncut, s_n64;
     const int nbra = *bra.n_rec;
     const int nket = *ket.n;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -72,53 +165,22 @@ coulomb_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double t
         const PairGeo b = load_geo(bra.geo, bra.sp_stride, sp);
         const double qb = __ldg(bra.rec_q + r);
         if (threadIdx.x == 0) {
-            // kets with qb * tmax * (1 + slack) > thr form a prefix (tmax descending)
-            int lo = 0, hi = nket;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (qb * __ldg(ket.tmax + mid) * (1.0 + SCREEN_SLACK) > thr) lo = mid + 1;
-                else hi = mid;
-            }
-            s_ncut = lo;
-            // screened-in shell quartets of this record (exact bound, no slack)
-            int lo2 = 0, hi2 = lo;
-            while (lo2 < hi2) {
-                const int mid = (lo2 + hi2) >> 1;
-                if (qb * __ldg(ket.tmax + mid) > thr) lo2 = mid + 1;
-                else hi2 = mid;
-            }
-            if (qcount) atomicAdd(qcount, (unsigned long long)lo2);
+            int ncut, nexact, n64;
+            ket_prefixes(ket, nket, qb, thr, fp32_cut, ncut, nexact, n64);
+            s_ncut = ncut;
+            s_n64 = n64;
+            if (qcount) atomicAdd(qcount, (unsigned long long)nexact);
         }
         __syncthreads();
-        const int ncut = s_ncut;
+        const int ncut = s_ncut, n64 = s_n64;
 
         double X[NE];
 #pragma unroll
         for (int e = 0; e < NE; e++) X[e] = 0.0;
-
-        for (int kt = threadIdx.x; kt < ncut; kt += J_THREADS) {
-            const PairGeo k = load_geo(ket.geo, ket.stride, kt);
-            QV q;
-            double F[L + 1];
-            make_quartet<L>(b, k, 0.0, boys_tab, q, F);
-            double Dpp[NF];
-            if (qb * __ldg(ket.tmin + kt) > thr * (1.0 + SCREEN_SLACK)) {
-#pragma unroll
-                for (int f = 0; f < NF; f++) Dpp[f] = __ldg(ket.Dpp + f * ket.stride + kt);
-            } else {
-                // exact per-component screen, same product order as the
-                // reference: fabs(Q_ij * Q_kl * D_kl) <= thr -> skip
-                double Dm[NCD];
-#pragma unroll
-                for (int c = 0; c < NCD; c++) {
-                    const double qk = __ldg(ket.Qc + c * ket.stride + kt);
-                    const double dk = __ldg(ket.Dc + c * ket.stride + kt);
-                    Dm[c] = (fabs(qb * qk * dk) > thr) ? __ldg(ket.Dm + c * ket.stride + kt) : 0.0;
-                }
-                hrr_ket_adjoint<LC, LD>(k.Rx, k.Ry, k.Rz, Dm, Dpp);
-            }
-            j_contract<LA, LB, LC, LD>(q, F, Dpp, X);
-        }
+        for (int kt = threadIdx.x; kt < n64; kt += J_THREADS)
+            j_quartet<LA, LB, LC, LD, double>(b, qb, ket, kt, thr, tabs, X);
+        for (int kt = n64 + threadIdx.x; kt < ncut; kt += J_THREADS)
+            j_quartet<LA, LB, LC, LD, float>(b, qb, ket, kt, thr, tabs, X);
 
 #pragma unroll
         for (int e = 0; e < NE; e++) {
@@ -136,7 +198,7 @@ coulomb_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double t
                 Xs[e] = s;
             }
             double J[NAB];
-            hrr_bra_vector<LA, LB>(b.Rx, b.Ry, b.Rz, Xs, J);
+            hrr_bra_vector<LA, LB, double>(b.Rx, b.Ry, b.Rz, Xs, J);
             const uint64_t mask = __ldg(bra.rec_mask + r);
 #pragma unroll
             for (int c = 0; c < NAB; c++) {
@@ -169,21 +231,135 @@ struct KPartnerRecs {
     int64_t sp_stride;
 };
 
-template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(K_THREADS)
-exchange_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd,
-                const uint32_t* __restrict__ b_aoinds, uint32_t b_count,
-                const uint32_t* __restrict__ d_aoinds, uint32_t d_count,
-                const double* __restrict__ Dao, uint32_t naos, double maxD, double omega, double thr,
-                double* __restrict__ mat_K, const double* __restrict__ boys_tab,
-                unsigned long long* __restrict__ qcount)
+struct KDensity {
+    const uint32_t* b_aoinds;
+    uint32_t b_count;
+    const uint32_t* d_aoinds;
+    uint32_t d_count;
+    const double* D;
+    uint32_t naos;
+};
+
+// Partner-pair enumeration of one chunk of j records of an output block:
+// nl[t] / n64[t] = passing / FP64 prefix lengths of the l list for j record
+// jb + t, then exclusive scans c64 (FP64 pairs) and c32 (FP32 pairs).
+struct KChunk {
+    int* nl;
+    int* n64;
+    int* c64;
+    int* c32;
+};
+
+__device__ __forceinline__ void k_chunk_scan(const KPartnerRecs& ab, const KPartnerRecs& cd, int jb, int nj, int c0,
+                                             int c1, double maxD, double thr, double fp32_cut, KChunk s)
+{
+    for (int t = threadIdx.x; t < nj; t += blockDim.x) {
+        const double qij = __ldg(ab.rec_q + jb + t);
+        int lo = c0, hi = c1;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (fabs(qij * __ldg(cd.rec_q + mid) * maxD) > thr) lo = mid + 1;
+            else hi = mid;
+        }
+        const int nl = lo - c0;
+        int n64 = nl;
+        if (fp32_cut > 0.0) {
+            int lo2 = c0, hi2 = lo;
+            while (lo2 < hi2) {
+                const int mid = (lo2 + hi2) >> 1;
+                if (fabs(qij * __ldg(cd.rec_q + mid) * maxD) >= fp32_cut) lo2 = mid + 1;
+                else hi2 = mid;
+            }
+            n64 = lo2 - c0;
+        }
+        s.nl[t] = nl;
+        s.n64[t] = n64;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s.c64[0] = 0;
+        s.c32[0] = 0;
+        for (int t = 0; t < nj; t++) {
+            s.c64[t + 1] = s.c64[t] + s.n64[t];
+            s.c32[t + 1] = s.c32[t] + (s.nl[t] - s.n64[t]);
+        }
+    }
+    __syncthreads();
+}
+
+// index t of the last entry with c[t] <= w (c ascending, c[0] = 0 <= w)
+__device__ __forceinline__ int k_find(const int* c, int n, int w)
+{
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (c[mid] <= w) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <int LA, int LB, int LC, int LD, typename T>
+__device__ __forceinline__ void k_quartet(const KPartnerRecs& ab, const KPartnerRecs& cd, int jr, int lr,
+                                          const KDensity& dm, double omega, const BoysTabs& tabs, double* Kacc)
 {
     constexpr int L = LA + LB + LC + LD;
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    const int spj = __ldg(ab.rec_sp + jr), spl = __ldg(cd.rec_sp + lr);
+    const PairGeo bg = load_geo(ab.geo, ab.sp_stride, spj);
+    const PairGeo kg = load_geo(cd.geo, cd.sp_stride, spl);
+    QVT<T> q;
+    T F[L + 1];
+    make_quartet_t<L>(bg, kg, omega, tabs.f64, tabs.f32, q, F);
+    T I[NA * NB * NC * ND];
+    eri_full<LA, LB, LC, LD, T>(q, F, I);
+    const int jsh = __ldg(ab.partner + spj), lsh = __ldg(cd.partner + spl);
+    T Dv[NB * ND];
+#pragma unroll
+    for (int cb = 0; cb < NB; cb++) {
+        const uint32_t jao = __ldg(dm.b_aoinds + jsh + (int64_t)dm.b_count * cb);
+#pragma unroll
+        for (int cdd = 0; cdd < ND; cdd++) {
+            const uint32_t lao = __ldg(dm.d_aoinds + lsh + (int64_t)dm.d_count * cdd);
+            Dv[cb * ND + cdd] = (T)__ldg(dm.D + (int64_t)jao * dm.naos + lao);
+        }
+    }
+    T Sij[NA * NB], Skl[NC * ND];
+    const uint64_t mj = __ldg(ab.rec_mask + jr), ml = __ldg(cd.rec_mask + lr);
+#pragma unroll
+    for (int x = 0; x < NA * NB; x++)
+        Sij[x] = ((mj >> x) & 1ull) ? (T)__ldg(ab.S + x * ab.sp_stride + spj) : (T)0;
+#pragma unroll
+    for (int x = 0; x < NC * ND; x++)
+        Skl[x] = ((ml >> x) & 1ull) ? (T)__ldg(cd.S + x * cd.sp_stride + spl) : (T)0;
+#pragma unroll
+    for (int ca = 0; ca < NA; ca++)
+#pragma unroll
+        for (int cc = 0; cc < NC; cc++) {
+            T acc = (T)0;
+#pragma unroll
+            for (int cb = 0; cb < NB; cb++) {
+                T s = (T)0;
+#pragma unroll
+                for (int cdd = 0; cdd < ND; cdd++)
+                    s = fma(I[((ca * NB + cb) * NC + cc) * ND + cdd] * Skl[cc * ND + cdd], Dv[cb * ND + cdd], s);
+                acc = fma(s, Sij[ca * NB + cb], acc);
+            }
+            Kacc[ca * NC + cc] += (double)acc;
+        }
+}
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(K_THREADS)
+exchange_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity dm, double maxD, double omega, double thr,
+                double* __restrict__ mat_K, BoysTabs tabs, unsigned long long* __restrict__ qcount, double fp32_cut)
+{
+    constexpr int NA = ncart(LA), NC = ncart(LC);
     constexpr int NAC = NA * NC;
     constexpr int NW = K_THREADS / 32;
-    __shared__ int s_cnt[K_JCHUNK + 1];
+    __shared__ int s_nl[K_JCHUNK], s_n64[K_JCHUNK], s_c64[K_JCHUNK + 1], s_c32[K_JCHUNK + 1];
     __shared__ double red[NW][NAC];
+    const KChunk ch{s_nl, s_n64, s_c64, s_c32};
     const int nout = *out.n;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -197,69 +373,17 @@ exchange_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd,
 
         for (int jb = a0; jb < a1; jb += K_JCHUNK) {
             const int nj = min(K_JCHUNK, a1 - jb);
-            for (int t = threadIdx.x; t < nj; t += K_THREADS) {
-                const double qij = __ldg(ab.rec_q + jb + t);
-                int lo = c0, hi = c1;
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if (fabs(qij * __ldg(cd.rec_q + mid) * maxD) > thr) lo = mid + 1;
-                    else hi = mid;
-                }
-                s_cnt[t + 1] = lo - c0;
+            k_chunk_scan(ab, cd, jb, nj, c0, c1, maxD, thr, fp32_cut, ch);
+            const int t64 = s_c64[nj], t32 = s_c32[nj];
+            if (qcount && threadIdx.x == 0) atomicAdd(qcount, (unsigned long long)(t64 + t32));
+            for (int w = threadIdx.x; w < t64; w += K_THREADS) {
+                const int jj = k_find(s_c64, nj, w);
+                k_quartet<LA, LB, LC, LD, double>(ab, cd, jb + jj, c0 + (w - s_c64[jj]), dm, omega, tabs, Kacc);
             }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                s_cnt[0] = 0;
-                for (int t = 1; t <= nj; t++) s_cnt[t] += s_cnt[t - 1];
-            }
-            __syncthreads();
-            const int total = s_cnt[nj];
-            if (qcount && threadIdx.x == 0) atomicAdd(qcount, (unsigned long long)total);
-            int jj = 0;
-            for (int w = threadIdx.x; w < total; w += K_THREADS) {
-                while (s_cnt[jj + 1] <= w) jj++;
-                const int jr = jb + jj;
-                const int lr = c0 + (w - s_cnt[jj]);
-                const int spj = __ldg(ab.rec_sp + jr), spl = __ldg(cd.rec_sp + lr);
-                const PairGeo bg = load_geo(ab.geo, ab.sp_stride, spj);
-                const PairGeo kg = load_geo(cd.geo, cd.sp_stride, spl);
-                QV q;
-                double F[L + 1];
-                make_quartet<L>(bg, kg, omega, boys_tab, q, F);
-                double I[NA * NB * NC * ND];
-                eri_full<LA, LB, LC, LD>(q, F, I);
-                const int jsh = __ldg(ab.partner + spj), lsh = __ldg(cd.partner + spl);
-                double Dv[NB * ND];
-#pragma unroll
-                for (int cb = 0; cb < NB; cb++) {
-                    const uint32_t jao = __ldg(b_aoinds + jsh + (int64_t)b_count * cb);
-#pragma unroll
-                    for (int cdd = 0; cdd < ND; cdd++) {
-                        const uint32_t lao = __ldg(d_aoinds + lsh + (int64_t)d_count * cdd);
-                        Dv[cb * ND + cdd] = __ldg(Dao + (int64_t)jao * naos + lao);
-                    }
-                }
-                double Sij[NA * NB], Skl[NC * ND];
-                const uint64_t mj = __ldg(ab.rec_mask + jr), ml = __ldg(cd.rec_mask + lr);
-#pragma unroll
-                for (int x = 0; x < NA * NB; x++)
-                    Sij[x] = ((mj >> x) & 1ull) ? __ldg(ab.S + x * ab.sp_stride + spj) : 0.0;
-#pragma unroll
-                for (int x = 0; x < NC * ND; x++)
-                    Skl[x] = ((ml >> x) & 1ull) ? __ldg(cd.S + x * cd.sp_stride + spl) : 0.0;
-#pragma unroll
-                for (int ca = 0; ca < NA; ca++)
-#pragma unroll
-                    for (int cb = 0; cb < NB; cb++)
-#pragma unroll
-                        for (int cc = 0; cc < NC; cc++) {
-                            double acc = 0.0;
-#pragma unroll
-                            for (int cdd = 0; cdd < ND; cdd++)
-                                acc = fma(I[((ca * NB + cb) * NC + cc) * ND + cdd] * Skl[cc * ND + cdd],
-                                          Dv[cb * ND + cdd], acc);
-                            Kacc[ca * NC + cc] = fma(acc, Sij[ca * NB + cb], Kacc[ca * NC + cc]);
-                        }
+            for (int w = threadIdx.x; w < t32; w += K_THREADS) {
+                const int jj = k_find(s_c32, nj, w);
+                k_quartet<LA, LB, LC, LD, float>(ab, cd, jb + jj, c0 + s_n64[jj] + (w - s_c32[jj]), dm, omega, tabs,
+                                                 Kacc);
             }
             __syncthreads();
         }

@@ -39,6 +39,43 @@ static void build_boys_host(std::vector<double>& tab)
 
 static std::mutex g_mu;
 static const double* g_boys_dev[64] = {nullptr};
+static const float* g_boys32_dev[64] = {nullptr};
+static std::atomic<double> g_fp32_cut{0.0};
+
+double fp32_cut_get() { return g_fp32_cut.load(std::memory_order_relaxed); }
+
+int fp32_cut_set(double cut)
+{
+    if (!(cut >= 0.0)) return VLXB_EINVAL;
+    g_fp32_cut.store(cut);
+    return VLXB_OK;
+}
+
+const float* boys_table32_device()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        if (g_boys32_dev[dev]) return g_boys32_dev[dev];
+    }
+    std::vector<double> host;
+    build_boys_host(host);
+    std::vector<float> h32(host.begin(), host.end());
+    float* d = nullptr;
+    if (cudaMalloc(&d, h32.size() * sizeof(float)) != cudaSuccess) return nullptr;
+    if (cudaMemcpy(d, h32.data(), h32.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(d);
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_boys32_dev[dev]) {
+        cudaFree(d);
+        return g_boys32_dev[dev];
+    }
+    g_boys32_dev[dev] = d;
+    return d;
+}
 static bool g_pool_done[64] = {false};
 static unsigned long long* g_counters[64] = {nullptr};
 

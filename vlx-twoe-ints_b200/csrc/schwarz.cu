@@ -37,7 +37,7 @@ schwarz_kernel(const double* __restrict__ info_a, uint32_t cnt_a, const double* 
         double F[L + 1];
         make_quartet<L>(g, g, 0.0, boys_tab, q, F);
         double I[NA * NB * NA * NB];
-        eri_full<LA, LB, LA, LB>(q, F, I);
+        eri_full<LA, LB, LA, LB, double>(q, F, I);
         double m = 0.0;
 #pragma unroll
         for (int c = 0; c < NA * NB; c++) m = fmax(m, fabs(I[c * NA * NB + c]));

@@ -75,6 +75,8 @@ class Lib:
         c.vlxb_getSchedule.argtypes = [ctypes.c_int] * 5
         c.vlxb_launchCount.argtypes = [ctypes.c_void_p, ctypes.c_int]
         c.vlxb_fp64Probe.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        c.vlxb_setFp32Cutoff.argtypes = [ctypes.c_double]
+        c.vlxb_getFp32Cutoff.restype = ctypes.c_double
 
     def check(self, rc: int, what: str):
         if rc != 0:
@@ -107,6 +109,13 @@ class Lib:
     def get_schedule(self, kind: str, cls: str) -> int:
         l = [{"s": 0, "p": 1, "d": 2}[x] for x in cls]
         return int(self.cdll.vlxb_getSchedule(0 if kind == "J" else 1, *l))
+
+    def set_fp32_cut(self, cutoff: float):
+        """Quartets with screening bound below `cutoff` run in FP32 (0 = FP64)."""
+        self.check(self.cdll.vlxb_setFp32Cutoff(float(cutoff)), "vlxb_setFp32Cutoff")
+
+    def get_fp32_cut(self) -> float:
+        return float(self.cdll.vlxb_getFp32Cutoff())
 
     def launch_count(self, reset: bool = False) -> int:
         out = ctypes.c_ulonglong(0)
