@@ -45,8 +45,11 @@ struct ExchangeArgs {
     double thr;
 };
 
+// Coulomb class call on a given arena (pool, static or measuring) with given
+// Boys tables and quartet counter (may be null).
 template <int LA, int LB, int LC, int LD>
-int run_coulomb(const CoulombArgs& a, cudaStream_t st)
+int run_coulomb_impl(const CoulombArgs& a, cudaStream_t st, Arena& ar, const BoysTabs& tab,
+                     unsigned long long* qc, double cut)
 {
     if (a.n_ab == 0 || a.n_cd == 0) return VLXB_OK;
     if (!a.mat_J || !a.cd_D || !a.ab_Q || !a.cd_Q || !a.ab_first || !a.ab_second || !a.ab_pdata || !a.cd_first ||
@@ -56,16 +59,11 @@ int run_coulomb(const CoulombArgs& a, cudaStream_t st)
     for (int t = 0; t < 4; t++)
         if (!a.info[L4[t]] || a.count[L4[t]] == 0) return VLXB_EINVAL;
     if (!(a.thr >= 0.0)) return VLXB_EINVAL;
-    int rc = ensure_pool_configured();
-    if (rc) return rc;
-    const BoysTabs tab{boys_table_device(), boys_table32_device()};
     if (!tab.f64 || !tab.f32) return VLXB_ECUDA;
-    const double cut = fp32_cut_get();
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-    Arena ar(st);
     PairGroups gb, gk;
-    rc = group_flat(ar, NA, NB, (int)a.count[LA], (int)a.count[LB], a.ab_first, a.ab_second, a.n_ab, a.info[LA],
-                    a.count[LA], a.info[LB], a.count[LB], gb);
+    int rc = group_flat(ar, NA, NB, (int)a.count[LA], (int)a.count[LB], a.ab_first, a.ab_second, a.n_ab,
+                        a.info[LA], a.count[LA], a.info[LB], a.count[LB], gb);
     if (rc) return rc;
     rc = make_records(ar, NA * NB, gb, a.ab_Q, a.n_ab);
     if (rc) return rc;
@@ -75,19 +73,31 @@ int run_coulomb(const CoulombArgs& a, cudaStream_t st)
     JKetData kd;
     rc = jket_prepare<LC, LD>(ar, gk, a.cd_first, a.cd_second, a.cd_D, a.cd_Q, a.cd_pdata, kd);
     if (rc) return rc;
+    if (ar.failed()) return VLXB_ENOMEM;
+    if (ar.measuring()) return VLXB_OK;
     JBraRecs bra{gb.rec_sp, gb.rec_q, gb.rec_mask, gb.n_rec, gb.geo, gb.entry, gb.sp_stride, a.ab_pdata};
     JKetPairs ket{kd.geo, kd.tmax, kd.tmin, kd.Dpp, kd.Dm, kd.Qc, kd.Dc, kd.stride, kd.n};
     int grid = launch_grid_limit();
     if ((int64_t)grid > (int64_t)a.n_ab) grid = (int)a.n_ab;
     if (schedule_get(0, LA, LB, LC, LD) == 1)
-        coulomb_col_kernel<LA, LB, LC, LD><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab,
-                                                                        quartet_counters_device(), cut);
+        coulomb_col_kernel<LA, LB, LC, LD><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut);
     else
-        coulomb_kernel<LA, LB, LC, LD><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab,
-                                                                    quartet_counters_device(), cut);
+        coulomb_kernel<LA, LB, LC, LD><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut);
     note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
+}
+
+template <int LA, int LB, int LC, int LD>
+int run_coulomb(const CoulombArgs& a, cudaStream_t st)
+{
+    if (a.n_ab == 0 || a.n_cd == 0) return VLXB_OK;
+    int rc = ensure_pool_configured();
+    if (rc) return rc;
+    const BoysTabs tab{boys_table_device(), boys_table32_device()};
+    if (!tab.f64 || !tab.f32) return VLXB_ECUDA;
+    Arena ar(st);
+    return run_coulomb_impl<LA, LB, LC, LD>(a, st, ar, tab, quartet_counters_device(), fp32_cut_get());
 }
 
 template <int LA, int LB, int LC, int LD>
@@ -135,8 +145,8 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
         if (rc) return rc;
     }
     KOutBlocks out{ko.ish, ko.ksh, ko.idx, ko.stride, ko.n};
-    KPartnerRecs rab{gab.rec_sp, gab.rec_q, gab.rec_mask, gab.seg, gab.geo, gab.S, gab.sp_j, gab.sp_stride};
-    KPartnerRecs rcd{gcd.rec_sp, gcd.rec_q, gcd.rec_mask, gcd.seg, gcd.geo, gcd.S, gcd.sp_j, gcd.sp_stride};
+    KPartnerRecs rab{gab.rec_sp, gab.rec_q, gab.rec_mask, gab.seg, gab.geo, gab.S, gab.sp_j, gab.sp_stride, gab.su};
+    KPartnerRecs rcd{gcd.rec_sp, gcd.rec_q, gcd.rec_mask, gcd.seg, gcd.geo, gcd.S, gcd.sp_j, gcd.sp_stride, gcd.su};
     int grid = launch_grid_limit();
     if ((int64_t)grid > (int64_t)a.n_ik) grid = (int)a.n_ik;
     unsigned long long* qc = quartet_counters_device();

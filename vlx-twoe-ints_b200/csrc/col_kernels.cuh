@@ -106,6 +106,8 @@ __device__ __forceinline__ void kcol_quartet(bool act, int jr, int lr, const KPa
     if (act) {
         const int jsh = __ldg(ab.partner + spj), lsh = __ldg(cd.partner + spl);
         const uint64_t mj = __ldg(ab.rec_mask + jr), ml = __ldg(cd.rec_mask + lr);
+        const double suj = __ldg(ab.su + jr), sul = __ldg(cd.su + lr);
+        const bool uni = !isnan(suj) && !isnan(sul);
 #pragma unroll
         for (int p = 0; p < NPASS; p++) {
             const int u = lig + NL * p;
@@ -118,48 +120,70 @@ __device__ __forceinline__ void kcol_quartet(bool act, int jr, int lr, const KPa
                     const int dd = u % ND;
                     T I[NA * NB];
                     hrr_bra_vector<LA, LB, T>(q.ABx, q.ABy, q.ABz, v, I);
-                    const double skl = ((ml >> u) & 1ull) ? __ldg(cd.S + u * cd.sp_stride + spl) : 0.0;
+                    const double skl =
+                        uni ? sul : (((ml >> u) & 1ull) ? __ldg(cd.S + u * cd.sp_stride + spl) : 0.0);
                     const uint32_t lao = __ldg(dm.d_aoinds + lsh + (int64_t)dm.d_count * dd);
                     T wv[NB];
 #pragma unroll
                     for (int b = 0; b < NB; b++) {
                         const uint32_t jao = __ldg(dm.b_aoinds + jsh + (int64_t)dm.b_count * b);
-                        wv[b] = (T)(skl * __ldg(dm.D + (int64_t)jao * dm.naos + lao));
+                        wv[b] = (T)((uni ? skl * suj : skl) * __ldg(dm.D + (int64_t)jao * dm.naos + lao));
                     }
+                    if (uni) {
 #pragma unroll
-                    for (int a = 0; a < NA; a++) {
-                        T s = (T)0;
+                        for (int a = 0; a < NA; a++) {
+                            T s = (T)0;
 #pragma unroll
-                        for (int b = 0; b < NB; b++) {
-                            const T sij = ((mj >> (a * NB + b)) & 1ull)
-                                              ? (T)__ldg(ab.S + (a * NB + b) * ab.sp_stride + spj) : (T)0;
-                            s = fma(I[a * NB + b] * sij, wv[b], s);
+                            for (int b = 0; b < NB; b++) s = fma(I[a * NB + b], wv[b], s);
+                            Kacc[p][a] += (double)s;
                         }
-                        Kacc[p][a] += (double)s;
+                    } else {
+#pragma unroll
+                        for (int a = 0; a < NA; a++) {
+                            T s = (T)0;
+#pragma unroll
+                            for (int b = 0; b < NB; b++) {
+                                const T sij = ((mj >> (a * NB + b)) & 1ull)
+                                                  ? (T)__ldg(ab.S + (a * NB + b) * ab.sp_stride + spj) : (T)0;
+                                s = fma(I[a * NB + b] * sij, wv[b], s);
+                            }
+                            Kacc[p][a] += (double)s;
+                        }
                     }
                 } else {
                     // unit = (a, b): ket HRR, then K[a][c] += Sij[ab] sum_d (ab|cd) Skl[cd] D[b][d]
                     const int bb = u % NB;
                     T I[NC * ND];
                     hrr_bra_vector<LC, LD, T>(q.CDx, q.CDy, q.CDz, v, I);
-                    const double sij = ((mj >> u) & 1ull) ? __ldg(ab.S + u * ab.sp_stride + spj) : 0.0;
+                    const double sij =
+                        uni ? suj : (((mj >> u) & 1ull) ? __ldg(ab.S + u * ab.sp_stride + spj) : 0.0);
                     const uint32_t jao = __ldg(dm.b_aoinds + jsh + (int64_t)dm.b_count * bb);
                     T wv[ND];
 #pragma unroll
                     for (int d = 0; d < ND; d++) {
                         const uint32_t lao = __ldg(dm.d_aoinds + lsh + (int64_t)dm.d_count * d);
-                        wv[d] = (T)(sij * __ldg(dm.D + (int64_t)jao * dm.naos + lao));
+                        wv[d] = (T)((uni ? sij * sul : sij) * __ldg(dm.D + (int64_t)jao * dm.naos + lao));
                     }
+                    if (uni) {
 #pragma unroll
-                    for (int c = 0; c < NC; c++) {
-                        T s = (T)0;
+                        for (int c = 0; c < NC; c++) {
+                            T s = (T)0;
 #pragma unroll
-                        for (int d = 0; d < ND; d++) {
-                            const T skl = ((ml >> (c * ND + d)) & 1ull)
-                                              ? (T)__ldg(cd.S + (c * ND + d) * cd.sp_stride + spl) : (T)0;
-                            s = fma(I[c * ND + d] * skl, wv[d], s);
+                            for (int d = 0; d < ND; d++) s = fma(I[c * ND + d], wv[d], s);
+                            Kacc[p][c] += (double)s;
                         }
-                        Kacc[p][c] += (double)s;
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < NC; c++) {
+                            T s = (T)0;
+#pragma unroll
+                            for (int d = 0; d < ND; d++) {
+                                const T skl = ((ml >> (c * ND + d)) & 1ull)
+                                                  ? (T)__ldg(cd.S + (c * ND + d) * cd.sp_stride + spl) : (T)0;
+                                s = fma(I[c * ND + d] * skl, wv[d], s);
+                            }
+                            Kacc[p][c] += (double)s;
+                        }
                     }
                 }
             }

@@ -14,6 +14,7 @@ enum Status : int {
     VLXB_EINVAL = 1,   // invalid argument (null pointer, bad count or class)
     VLXB_ECUDA = 2,    // a CUDA runtime call failed
     VLXB_ENOMEM = 3,   // device allocation failed
+    VLXB_ETOOBIG = 4,  // the call needs more scratch than a fixed buffer holds
 };
 
 #define VLXB_CHECK_CUDA(call)                              \
@@ -22,13 +23,20 @@ enum Status : int {
         if (_e != cudaSuccess) return (_e == cudaErrorMemoryAllocation) ? VLXB_ENOMEM : VLXB_ECUDA; \
     } while (0)
 
-// Stream-ordered scratch arena: every buffer is taken from the device's
-// default memory pool with cudaMallocAsync on the call's stream and handed
-// back with cudaFreeAsync when the arena goes out of scope, so scratch is
-// reused across calls without synchronisation.
+// Scratch arena of one call.  Pool mode (default): every buffer is taken
+// from the device's default memory pool with cudaMallocAsync on the call's
+// stream and handed back with cudaFreeAsync when the arena goes out of scope,
+// so scratch is reused across calls without synchronisation.  Static mode:
+// buffers are carved (256-byte aligned) out of a fixed device buffer given by
+// the caller, nothing is allocated.  Measure mode: nothing is allocated or
+// launched; alloc only adds up the bytes a static-mode call would need (the
+// pointers it returns must not be used), and every launch site skips its
+// launch (see VLXB_RUN).
 class Arena {
   public:
     explicit Arena(cudaStream_t s) : stream_(s) {}
+    Arena(cudaStream_t s, char* base, size_t cap, bool measure)
+        : stream_(s), base_(base), cap_(cap), static_(true), measure_(measure) {}
     ~Arena()
     {
         for (void* p : ptrs_) cudaFreeAsync(p, stream_);
@@ -40,8 +48,18 @@ class Arena {
     T* alloc(int64_t n)
     {
         if (failed_) return nullptr;
-        void* p = nullptr;
         size_t bytes = (size_t)(n > 0 ? n : 1) * sizeof(T);
+        if (static_) {
+            const size_t off = (used_ + 255) & ~(size_t)255;
+            used_ = off + bytes;
+            if (measure_) return (T*)(uintptr_t)(256 + off);  // placeholder, never dereferenced
+            if (used_ > cap_) {
+                failed_ = true;
+                return nullptr;
+            }
+            return (T*)(base_ + off);
+        }
+        void* p = nullptr;
         if (cudaMallocAsync(&p, bytes, stream_) != cudaSuccess) {
             failed_ = true;
             cudaGetLastError();
@@ -51,18 +69,35 @@ class Arena {
         return (T*)p;
     }
     bool failed() const { return failed_; }
+    bool measuring() const { return measure_; }
+    size_t used() const { return used_; }
     cudaStream_t stream() const { return stream_; }
 
   private:
     cudaStream_t stream_;
     std::vector<void*> ptrs_;
+    char* base_ = nullptr;
+    size_t cap_ = 0, used_ = 0;
+    bool static_ = false, measure_ = false;
     bool failed_ = false;
 };
+
+// Launches, memsets and CUB runs go through VLXB_RUN so that a measuring
+// arena only sizes the call.
+#define VLXB_RUN(ar, ...)            \
+    do {                             \
+        if (!(ar).measuring()) {     \
+            __VA_ARGS__;             \
+        }                            \
+    } while (0)
 
 // Per-device FP64 Boys table (BOYS_NGRID x BOYS_NCOL), built on first use.
 // Returns nullptr on failure.  The first call on a device synchronises it
 // (table upload); call vlxb_init() before any stream capture.
 const double* boys_table_device();
+
+// Host copy of the FP64 Boys table (BOYS_NGRID x BOYS_NCOL values).
+void boys_host_table(std::vector<double>& tab);
 
 // Float copy of the same table for the mixed-precision path.
 const float* boys_table32_device();
@@ -96,6 +131,7 @@ struct PairGroups {
     uint64_t* rec_mask = nullptr;
     int* seg = nullptr;        // [npa + 1] (segmented records only)
     double* S = nullptr;       // [NXY][sp_stride] (partner records only)
+    double* su = nullptr;      // [rec_stride] uniform S of a record or NaN (partner records only)
 };
 
 // Group a flat list of prim-cart pairs (first[e], second[e]) by shell pair.

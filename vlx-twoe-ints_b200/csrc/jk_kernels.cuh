@@ -229,6 +229,7 @@ struct KPartnerRecs {
     const double* S;           // [NXY][sp_stride] S_ij_00 (0 where absent)
     const int32_t* partner;    // [sp_stride] partner primitive shell (j or l)
     int64_t sp_stride;
+    const double* su;          // [n_rec] S shared by all components of the record, or NaN
 };
 
 struct KDensity {
@@ -323,6 +324,24 @@ __device__ __forceinline__ void k_quartet(const KPartnerRecs& ab, const KPartner
             const uint32_t lao = __ldg(dm.d_aoinds + lsh + (int64_t)dm.d_count * cdd);
             Dv[cb * ND + cdd] = (T)__ldg(dm.D + (int64_t)jao * dm.naos + lao);
         }
+    }
+    const double suj = __ldg(ab.su + jr), sul = __ldg(cd.su + lr);
+    if (!isnan(suj) && !isnan(sul)) {
+        // every component of both records shares one S: K[a][c] += Sij Skl sum_bd (ab|cd) D[b][d]
+        const T fs = (T)(suj * sul);
+#pragma unroll
+        for (int ca = 0; ca < NA; ca++)
+#pragma unroll
+            for (int cc = 0; cc < NC; cc++) {
+                T acc = (T)0;
+#pragma unroll
+                for (int cb = 0; cb < NB; cb++)
+#pragma unroll
+                    for (int cdd = 0; cdd < ND; cdd++)
+                        acc = fma(I[((ca * NB + cb) * NC + cc) * ND + cdd], Dv[cb * ND + cdd], acc);
+                Kacc[ca * NC + cc] += (double)(acc * fs);
+            }
+        return;
     }
     T Sij[NA * NB], Skl[NC * ND];
     const uint64_t mj = __ldg(ab.rec_mask + jr), ml = __ldg(cd.rec_mask + lr);

@@ -37,6 +37,8 @@ static void build_boys_host(std::vector<double>& tab)
     }
 }
 
+void boys_host_table(std::vector<double>& tab) { build_boys_host(tab); }
+
 static std::mutex g_mu;
 static const double* g_boys_dev[64] = {nullptr};
 static const float* g_boys32_dev[64] = {nullptr};
@@ -178,7 +180,9 @@ static int scan_int(Arena& ar, const int* in, int* out, int64_t n)
     VLXB_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, (int)n, ar.stream()));
     void* tmp = ar.alloc<char>((int64_t)bytes);
     if (!tmp) return VLXB_ENOMEM;
-    VLXB_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, (int)n, ar.stream()));
+    if (!ar.measuring()) {
+        VLXB_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, (int)n, ar.stream()));
+    }
     return VLXB_OK;
 }
 
@@ -190,8 +194,10 @@ static int finish_grouping(Arena& ar, int64_t ntab, int* table, PairGroups& g)
     if (!g.spidx || !g.n_sp) return VLXB_ENOMEM;
     int rc = scan_int(ar, table, g.spidx, ntab);
     if (rc) return rc;
-    k_scan_total<<<1, 1, 0, st>>>(g.spidx, table, ntab, g.n_sp);
-    note_launches();
+    if (!ar.measuring()) {
+        k_scan_total<<<1, 1, 0, st>>>(g.spidx, table, ntab, g.n_sp);
+    }
+    if (!ar.measuring()) note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }
@@ -203,7 +209,9 @@ static int alloc_sp(Arena& ar, int nxy, PairGroups& g)
     g.entry = ar.alloc<int32_t>(g.sp_stride * nxy);
     g.geo = ar.alloc<double>(g.sp_stride * GEO_N);
     if (ar.failed()) return VLXB_ENOMEM;
-    VLXB_CHECK_CUDA(cudaMemsetAsync(g.entry, 0xFF, sizeof(int32_t) * g.sp_stride * nxy, ar.stream()));
+    if (!ar.measuring()) {
+        VLXB_CHECK_CUDA(cudaMemsetAsync(g.entry, 0xFF, sizeof(int32_t) * g.sp_stride * nxy, ar.stream()));
+    }
     return VLXB_OK;
 }
 
@@ -215,21 +223,29 @@ int group_flat(Arena& ar, int na, int nb, int npa, int npb, const uint32_t* firs
     const int64_t ntab = (int64_t)npa * npb;
     int* table = ar.alloc<int>(ntab);
     if (!table) return VLXB_ENOMEM;
-    VLXB_CHECK_CUDA(cudaMemsetAsync(table, 0, sizeof(int) * ntab, st));
-    k_mark_pairs<<<prep_blocks(n), PREP_THREADS, 0, st>>>(first, second, n, na, nb, npb, table);
-    note_launches();
+    if (!ar.measuring()) {
+        VLXB_CHECK_CUDA(cudaMemsetAsync(table, 0, sizeof(int) * ntab, st));
+    }
+    if (!ar.measuring()) {
+        k_mark_pairs<<<prep_blocks(n), PREP_THREADS, 0, st>>>(first, second, n, na, nb, npb, table);
+    }
+    if (!ar.measuring()) note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     int rc = finish_grouping(ar, ntab, table, g);
     if (rc) return rc;
     g.sp_stride = n < ntab ? n : ntab;
     rc = alloc_sp(ar, na * nb, g);
     if (rc) return rc;
-    k_fill_pairs<<<prep_blocks(n), PREP_THREADS, 0, st>>>(first, second, n, na, nb, npb, g.spidx, g.entry, g.sp_i,
-                                                          g.sp_j, g.sp_stride);
-    note_launches();
-    k_pair_geo<<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.sp_i, g.sp_j, info_a, cnt_a, info_b,
-                                                                   cnt_b, g.geo, g.sp_stride);
-    note_launches();
+    if (!ar.measuring()) {
+        k_fill_pairs<<<prep_blocks(n), PREP_THREADS, 0, st>>>(first, second, n, na, nb, npb, g.spidx, g.entry, g.sp_i,
+                                                              g.sp_j, g.sp_stride);
+    }
+    if (!ar.measuring()) note_launches();
+    if (!ar.measuring()) {
+        k_pair_geo<<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.sp_i, g.sp_j, info_a, cnt_a, info_b,
+                                                                       cnt_b, g.geo, g.sp_stride);
+    }
+    if (!ar.measuring()) note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }
@@ -243,21 +259,29 @@ int group_csr(Arena& ar, int na, int nb, int npa, int npb, const uint32_t* displ
     const int n_first = npa * na;
     int* table = ar.alloc<int>(ntab);
     if (!table) return VLXB_ENOMEM;
-    VLXB_CHECK_CUDA(cudaMemsetAsync(table, 0, sizeof(int) * ntab, st));
-    k_mark_csr<<<prep_blocks(n_first), PREP_THREADS, 0, st>>>(displs, counts, Dinds, n_first, na, nb, npb, table);
-    note_launches();
+    if (!ar.measuring()) {
+        VLXB_CHECK_CUDA(cudaMemsetAsync(table, 0, sizeof(int) * ntab, st));
+    }
+    if (!ar.measuring()) {
+        k_mark_csr<<<prep_blocks(n_first), PREP_THREADS, 0, st>>>(displs, counts, Dinds, n_first, na, nb, npb, table);
+    }
+    if (!ar.measuring()) note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     int rc = finish_grouping(ar, ntab, table, g);
     if (rc) return rc;
     g.sp_stride = n_entries_bound < ntab ? n_entries_bound : ntab;
     rc = alloc_sp(ar, na * nb, g);
     if (rc) return rc;
-    k_fill_csr<<<prep_blocks(n_first), PREP_THREADS, 0, st>>>(displs, counts, Dinds, n_first, na, nb, npb, g.spidx,
-                                                              g.entry, g.sp_i, g.sp_j, g.sp_stride);
-    note_launches();
-    k_pair_geo<<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.sp_i, g.sp_j, info_a, cnt_a, info_b,
-                                                                   cnt_b, g.geo, g.sp_stride);
-    note_launches();
+    if (!ar.measuring()) {
+        k_fill_csr<<<prep_blocks(n_first), PREP_THREADS, 0, st>>>(displs, counts, Dinds, n_first, na, nb, npb, g.spidx,
+                                                                  g.entry, g.sp_i, g.sp_j, g.sp_stride);
+    }
+    if (!ar.measuring()) note_launches();
+    if (!ar.measuring()) {
+        k_pair_geo<<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.sp_i, g.sp_j, info_a, cnt_a, info_b,
+                                                                       cnt_b, g.geo, g.sp_stride);
+    }
+    if (!ar.measuring()) note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }
@@ -265,20 +289,31 @@ int group_csr(Arena& ar, int na, int nb, int npa, int npb, const uint32_t* displ
 template <int NXY>
 static void launch_rec_count(const PairGroups& g, const double* Q, int* nrec, cudaStream_t st)
 {
-    k_rec_count<NXY><<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, g.sp_stride, Q, nrec);
+    {
+        k_rec_count<NXY><<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, g.sp_stride, Q, nrec);
+    }
     note_launches();
 }
 template <int NXY>
 static void launch_rec_fill(const PairGroups& g, const double* Q, const int* recoff, cudaStream_t st)
 {
-    k_rec_fill<NXY><<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, g.sp_stride, Q, recoff,
-                                                                       g.rec_sp, g.rec_q, g.rec_mask);
+    {
+        k_rec_fill<NXY><<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, g.sp_stride, Q, recoff,
+                                                                           g.rec_sp, g.rec_q, g.rec_mask);
+    }
     note_launches();
 }
 template <int NXY>
 static void launch_sp_S(const PairGroups& g, const double* pdata, cudaStream_t st)
 {
-    k_sp_S<NXY><<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, g.sp_stride, pdata, g.S);
+    {
+        k_sp_S<NXY><<<prep_blocks(g.sp_stride), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, g.sp_stride, pdata, g.S);
+    }
+    note_launches();
+    {
+        k_rec_uniform_s<NXY><<<prep_blocks(g.rec_stride), PREP_THREADS, 0, st>>>(g.n_rec, g.rec_sp, g.rec_mask, g.S,
+                                                                                 g.sp_stride, g.su);
+    }
     note_launches();
 }
 
@@ -306,14 +341,22 @@ int make_records(Arena& ar, int nxy, PairGroups& g, const double* Q, int64_t n_e
     g.rec_q = ar.alloc<double>(g.rec_stride);
     g.rec_mask = ar.alloc<uint64_t>(g.rec_stride);
     if (ar.failed()) return VLXB_ENOMEM;
-    VLXB_CHECK_CUDA(cudaMemsetAsync(nrec, 0, sizeof(int) * (g.sp_stride + 1), st));
-    VLXB_NXY_DISPATCH(nxy, launch_rec_count, g, Q, nrec, st);
+    if (!ar.measuring()) {
+        VLXB_CHECK_CUDA(cudaMemsetAsync(nrec, 0, sizeof(int) * (g.sp_stride + 1), st));
+    }
+    if (!ar.measuring()) {
+        VLXB_NXY_DISPATCH(nxy, launch_rec_count, g, Q, nrec, st);
+    }
     VLXB_CHECK_CUDA(cudaGetLastError());
     int rc = scan_int(ar, nrec, recoff, g.sp_stride + 1);
     if (rc) return rc;
-    k_scan_total<<<1, 1, 0, st>>>(recoff, nrec, g.sp_stride + 1, g.n_rec);
-    note_launches();
-    VLXB_NXY_DISPATCH(nxy, launch_rec_fill, g, Q, recoff, st);
+    if (!ar.measuring()) {
+        k_scan_total<<<1, 1, 0, st>>>(recoff, nrec, g.sp_stride + 1, g.n_rec);
+    }
+    if (!ar.measuring()) note_launches();
+    if (!ar.measuring()) {
+        VLXB_NXY_DISPATCH(nxy, launch_rec_fill, g, Q, recoff, st);
+    }
     VLXB_CHECK_CUDA(cudaGetLastError());
     // keep recoff for segment offsets
     g.seg = recoff;  // temporarily: record offsets per shell pair
@@ -331,11 +374,16 @@ int segment_records(Arena& ar, int nxy, int npa, int npb, PairGroups& g, const d
     int32_t* sp_sorted = ar.alloc<int32_t>(g.rec_stride);
     uint64_t* mask_sorted = ar.alloc<uint64_t>(g.rec_stride);
     g.S = ar.alloc<double>(g.sp_stride * nxy);
+    g.su = ar.alloc<double>(g.rec_stride);
     if (ar.failed()) return VLXB_ENOMEM;
-    k_rec_segments<<<prep_blocks(npa + 1), PREP_THREADS, 0, st>>>(g.spidx, recoff, npa, npb, g.n_rec, seg);
-    note_launches();
-    k_iota<<<prep_blocks(g.rec_stride), PREP_THREADS, 0, st>>>(perm_in, g.rec_stride);
-    note_launches();
+    if (!ar.measuring()) {
+        k_rec_segments<<<prep_blocks(npa + 1), PREP_THREADS, 0, st>>>(g.spidx, recoff, npa, npb, g.n_rec, seg);
+    }
+    if (!ar.measuring()) note_launches();
+    if (!ar.measuring()) {
+        k_iota<<<prep_blocks(g.rec_stride), PREP_THREADS, 0, st>>>(perm_in, g.rec_stride);
+    }
+    if (!ar.measuring()) note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     size_t bytes = 0;
     VLXB_CHECK_CUDA(cub::DeviceSegmentedRadixSort::SortPairsDescending(
@@ -344,15 +392,19 @@ int segment_records(Arena& ar, int nxy, int npa, int npb, PairGroups& g, const d
     if (!tmp) return VLXB_ENOMEM;
     VLXB_CHECK_CUDA(cub::DeviceSegmentedRadixSort::SortPairsDescending(
         tmp, bytes, g.rec_q, q_sorted, perm_in, perm, (int)g.rec_stride, npa, seg, seg + 1, 0, 64, st));
-    k_gather_recs<<<prep_blocks(g.rec_stride), PREP_THREADS, 0, st>>>(g.n_rec, perm, g.rec_sp, g.rec_mask,
-                                                                       sp_sorted, mask_sorted);
-    note_launches();
+    if (!ar.measuring()) {
+        k_gather_recs<<<prep_blocks(g.rec_stride), PREP_THREADS, 0, st>>>(g.n_rec, perm, g.rec_sp, g.rec_mask,
+                                                                           sp_sorted, mask_sorted);
+    }
+    if (!ar.measuring()) note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     g.rec_q = q_sorted;
     g.rec_sp = sp_sorted;
     g.rec_mask = mask_sorted;
     g.seg = seg;
-    VLXB_NXY_DISPATCH(nxy, launch_sp_S, g, pdata, st);
+    if (!ar.measuring()) {
+        VLXB_NXY_DISPATCH(nxy, launch_sp_S, g, pdata, st);
+    }
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }
@@ -383,23 +435,31 @@ int jket_prepare(Arena& ar, const PairGroups& g, const uint32_t* first, const ui
     if (ar.failed()) return VLXB_ENOMEM;
     out.stride = S;
     out.n = g.n_sp;
-    k_jket_fill<LC, LD><<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, S, first, second, D, Q, pdata,
-                                                                 g.geo, keys, tmin_u, Dpp_u, Dm_u, Qc_u, Dc_u, S);
-    note_launches();
-    k_iota<<<prep_blocks(S), PREP_THREADS, 0, st>>>(perm_in, S);
-    note_launches();
+    if (!ar.measuring()) {
+        k_jket_fill<LC, LD><<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, S, first, second, D, Q, pdata,
+                                                                     g.geo, keys, tmin_u, Dpp_u, Dm_u, Qc_u, Dc_u, S);
+    }
+    if (!ar.measuring()) note_launches();
+    if (!ar.measuring()) {
+        k_iota<<<prep_blocks(S), PREP_THREADS, 0, st>>>(perm_in, S);
+    }
+    if (!ar.measuring()) note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     size_t bytes = 0;
     VLXB_CHECK_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, keys, keys_sorted, perm_in, perm,
                                                               (int)S, 0, 64, st));
     void* tmp = ar.alloc<char>((int64_t)bytes);
     if (!tmp) return VLXB_ENOMEM;
-    VLXB_CHECK_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp, bytes, keys, keys_sorted, perm_in, perm, (int)S,
-                                                              0, 64, st));
-    k_jket_gather<LC, LD><<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, perm, S, g.geo, keys_sorted, tmin_u,
-                                                                   Dpp_u, Dm_u, Qc_u, Dc_u, out.geo, out.tmax,
-                                                                   out.tmin, out.Dpp, out.Dm, out.Qc, out.Dc);
-    note_launches();
+    if (!ar.measuring()) {
+        VLXB_CHECK_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp, bytes, keys, keys_sorted, perm_in, perm, (int)S,
+                                                                  0, 64, st));
+    }
+    if (!ar.measuring()) {
+        k_jket_gather<LC, LD><<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, perm, S, g.geo, keys_sorted, tmin_u,
+                                                                       Dpp_u, Dm_u, Qc_u, Dc_u, out.geo, out.tmax,
+                                                                       out.tmin, out.Dpp, out.Dm, out.Qc, out.Dc);
+    }
+    if (!ar.measuring()) note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }
@@ -421,8 +481,10 @@ template <int NAC>
 static void launch_kout(const uint32_t* pi, const uint32_t* pk, int64_t n, int na, int nc, int npc, const int* spidx,
                         KOutData& out, cudaStream_t st)
 {
-    k_kout_fill<NAC><<<prep_blocks(n), PREP_THREADS, 0, st>>>(pi, pk, n, na, nc, npc, spidx, out.idx, out.ish,
-                                                              out.ksh, out.stride);
+    {
+        k_kout_fill<NAC><<<prep_blocks(n), PREP_THREADS, 0, st>>>(pi, pk, n, na, nc, npc, spidx, out.idx, out.ish,
+                                                                  out.ksh, out.stride);
+    }
     note_launches();
 }
 
@@ -433,9 +495,13 @@ int kout_prepare(Arena& ar, int na, int nc, int npa, int npc, const uint32_t* pi
     const int64_t ntab = (int64_t)npa * npc;
     int* table = ar.alloc<int>(ntab);
     if (!table) return VLXB_ENOMEM;
-    VLXB_CHECK_CUDA(cudaMemsetAsync(table, 0, sizeof(int) * ntab, st));
-    k_mark_pairs<<<prep_blocks(n), PREP_THREADS, 0, st>>>(pi, pk, n, na, nc, npc, table);
-    note_launches();
+    if (!ar.measuring()) {
+        VLXB_CHECK_CUDA(cudaMemsetAsync(table, 0, sizeof(int) * ntab, st));
+    }
+    if (!ar.measuring()) {
+        k_mark_pairs<<<prep_blocks(n), PREP_THREADS, 0, st>>>(pi, pk, n, na, nc, npc, table);
+    }
+    if (!ar.measuring()) note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     PairGroups g;
     int rc = finish_grouping(ar, ntab, table, g);
@@ -446,8 +512,12 @@ int kout_prepare(Arena& ar, int na, int nc, int npa, int npc, const uint32_t* pi
     out.ksh = ar.alloc<int32_t>(out.stride);
     out.idx = ar.alloc<int32_t>(out.stride * na * nc);
     if (ar.failed()) return VLXB_ENOMEM;
-    VLXB_CHECK_CUDA(cudaMemsetAsync(out.idx, 0xFF, sizeof(int32_t) * out.stride * na * nc, st));
-    VLXB_NXY_DISPATCH(na * nc, launch_kout, pi, pk, n, na, nc, npc, g.spidx, out, st);
+    if (!ar.measuring()) {
+        VLXB_CHECK_CUDA(cudaMemsetAsync(out.idx, 0xFF, sizeof(int32_t) * out.stride * na * nc, st));
+    }
+    if (!ar.measuring()) {
+        VLXB_NXY_DISPATCH(na * nc, launch_kout, pi, pk, n, na, nc, npc, g.spidx, out, st);
+    }
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }

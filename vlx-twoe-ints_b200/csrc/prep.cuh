@@ -192,6 +192,29 @@ __global__ void k_sp_S(const int* __restrict__ n_sp, const int32_t* __restrict__
         }
 }
 
+// su[r] = the S shared by all components of record r when the record covers
+// every component of its shell pair and they share one S value, else NaN
+// (the kernels then digest with per-component S).
+template <int NXY>
+__global__ void k_rec_uniform_s(const int* __restrict__ n_rec, const int32_t* __restrict__ rec_sp,
+                                const uint64_t* __restrict__ rec_mask, const double* __restrict__ S, int64_t stride,
+                                double* __restrict__ su)
+{
+    const int n = *n_rec;
+    const uint64_t full = (NXY >= 64) ? ~0ull : ((1ull << NXY) - 1ull);
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const int sp = rec_sp[r];
+        double v = __longlong_as_double(0x7ff8000000000000ll);
+        if (rec_mask[r] == full) {
+            const double s0 = S[sp];
+            bool same = true;
+            for (int c = 1; c < NXY; c++) same &= (S[c * stride + sp] == s0);
+            if (same) v = s0;
+        }
+        su[r] = v;
+    }
+}
+
 // Segment offsets of records by first shell: seg[i] = recoff[spidx[i * npb]],
 // seg[np_first] = total records.
 __global__ void k_rec_segments(const int* __restrict__ spidx, const int* __restrict__ recoff, int np_first, int npb,

@@ -23,14 +23,23 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_SCHEDULE = os.path.join(HERE, "schedule_b200.json")
 
 
+# Thread-per-quartet kernels whose code does not fit in registers (ptxas
+# keeps them at 32 registers with 15-87 KB of local memory per thread); they
+# are 5-10x slower than the column kernels and are not timed.
+SPILLING_THREAD_KERNELS = {
+    "J": {"dddd"},
+    "K": {"ddds", "dpdp", "ppdd", "pddp", "sddd", "pdpd", "dpdd", "dddp", "pddd", "dddd"},
+}
+
+
 def compiled_variants(kind: str, cls: str):
     sys.path.insert(0, os.path.join(os.path.dirname(HERE), "csrc"))
     from gen_column import ColumnPlan, k_smem_bytes
 
     if kind == "J":
-        return [0, 1]
+        return [1] if cls in SPILLING_THREAD_KERNELS["J"] else [0, 1]
     l = [{"s": 0, "p": 1, "d": 2}[x] for x in cls]
-    out = [0]
+    out = [] if cls in SPILLING_THREAD_KERNELS["K"] else [0]
     for ori in (0, 1):
         if k_smem_bytes(ColumnPlan(*l, ori)) <= 46 * 1024:
             out.append(1 + ori)
