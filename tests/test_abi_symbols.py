@@ -18,9 +18,10 @@ def declared():
 
 def test_header_lists_all_reference_classes():
     names = declared()
-    j = [n for n in names if n.startswith("vlxb_computeCoulombFock")]
+    j = [n for n in names if n.startswith("vlxb_computeCoulombFock") and not n.endswith("_noalloc")]
     k = [n for n in names if n.startswith("vlxb_computeExchangeFock")]
     assert len(j) == 36 and len(k) == 54
+    assert [n for n in names if n.endswith("_noalloc")] == ["vlxb_computeCoulombFockSSSS_noalloc"]
     assert "vlxb_computeCoulombFockDDDD" in j and "vlxb_computeExchangeFockSDPD" in k and "vlxb_computeExchangeFockPDSD" not in k
 
 

@@ -52,6 +52,7 @@ const char* vlxb_status_string(int status)
         case VLXB_EINVAL: return "invalid argument";
         case VLXB_ECUDA: return "CUDA runtime error";
         case VLXB_ENOMEM: return "device memory allocation failed";
+        case VLXB_ETOOBIG: return "the call needs more scratch than the fixed no-allocation buffer holds";
         default: return "unknown status";
     }
 }

@@ -107,7 +107,8 @@ def header():
          " */",
          "#ifndef VLXB_H", "#define VLXB_H", "", "#include <stdint.h>", "",
          "#ifdef __cplusplus", 'extern "C" {', "#endif", "",
-         "#define VLXB_OK 0", "#define VLXB_EINVAL 1", "#define VLXB_ECUDA 2", "#define VLXB_ENOMEM 3", "",
+         "#define VLXB_OK 0", "#define VLXB_EINVAL 1", "#define VLXB_ECUDA 2", "#define VLXB_ENOMEM 3",
+         "#define VLXB_ETOOBIG 4", "",
          "/* Select `device`, configure its memory pool and upload the Boys table.",
          "   Call once per device before any stream capture.  No reference",
          "   counterpart (the reference's caller owns its Boys table). */",
@@ -153,7 +154,20 @@ def header():
          "   0 (the default) = plain FP64, the drop-in behaviour.  Process-wide.",
          "   No reference counterpart. */",
          "int vlxb_setFp32Cutoff(double cutoff);",
-         "double vlxb_getFp32Cutoff(void);", ""]
+         "double vlxb_getFp32Cutoff(void);", "",
+         "/* Allocation-free variant of vlxb_computeCoulombFockSSSS (same arguments,",
+         "   same result) for callers that cannot allocate device memory, e.g. hosts",
+         "   whose device memory is owned by their own allocator, or plugins that are",
+         "   not allowed to allocate.  No counterpart in the reference: the reference's",
+         "   emitted kernels need no scratch, this engine's entry points do.  Scratch",
+         "   comes from a fixed device array of VLXB_NOALLOC_SCRATCH_BYTES (64 MiB) that",
+         "   every GPU loading the library holds until exit; calls needing more",
+         "   return VLXB_ETOOBIG before queuing any work.  The first call on a device",
+         "   resolves the array and uploads the Boys tables (synchronously): make it",
+         "   before any stream capture.  Calls share the array, so calls that overlap",
+         "   on the GPU race; serialise them. */",
+         "#define VLXB_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)",
+         "int vlxb_computeCoulombFockSSSS_noalloc(" + ", ".join(j_params("ssss")) + ");", ""]
     L.append("/* ---- Coulomb: replace computeCoulombFock<ABCD> of gen_coulomb.py:74-93 ---- */")
     for cls in j_classes():
         L.append(f"/* replaces computeCoulombFock{cls.upper()} (gen_coulomb.py:74-93; class list gen_coulomb.py:47-56) */")
