@@ -238,7 +238,7 @@ def _k_variants(cls):
     out = [0]
     for ori in (0, 1):
         if k_smem_bytes(ColumnPlan(*l, ori)) <= 46 * 1024:
-            out.append(1 + ori)
+            out += [1 + ori, 3 + ori]
     return out
 
 
@@ -266,10 +266,11 @@ def test_golden_every_coulomb_variant(golden, variant):
             L.set_schedule("J", c, v)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 def test_golden_every_exchange_variant(golden, variant):
-    """All exchange kernels (thread per quartet; column with bra or ket lanes)
-    on every class where the variant is compiled."""
+    """All exchange kernels (thread per quartet; column with bra or ket lanes;
+    the same with contracted partners) on every class where the variant is
+    compiled."""
     z = golden
     L = lib()
     saved = {c: L.get_schedule("K", c) for c in tf.k_classes()}
@@ -325,3 +326,35 @@ def test_mixed_precision_errors_within_tolerance():
         L.set_fp32_cut(0.0)
     J2 = lists.contract_J(rl, {k: v.cpu().numpy() for k, v in mJ.items()})
     assert np.abs(J2 - Jo).max() <= 1e-4 * np.abs(Jo).max()
+
+
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
+def test_contracted_exchange_variants_vs_oracle(variant):
+    """Degree-3 contracted s/p/d shells (partner groups of up to 3 primitives
+    with one S per record): every exchange class through one kernel variant
+    against the FP64 oracle, also with range separation, and the quartet
+    counter equal to the record-by-record variant's."""
+    L = lib()
+    L.init(0)
+    wl = basis.config_custom(3, 4.0, {0: 2, 1: 1, 2: 1}, 3, 0.2, 2.5, 3, 1e-12, 17)
+    rl = lists.build_lists(wl.mol, wl.D, wl.threshold, fock.gpu_schwarz_fn())
+    dl = fock.to_device(rl)
+    saved = {c: L.get_schedule("K", c) for c in lists.k_classes()}
+    try:
+        for omega in (0.0, 0.4):
+            counts = {}
+            for v in (1, variant) if variant != 1 else (1,):
+                for c in lists.k_classes():
+                    L.set_schedule("K", c, v if v in _k_variants(c) else 0)
+                L.reset_counters()
+                _, mK = fock.build_jk(dl, omega=omega, do_j=False)
+                torch.cuda.synchronize()
+                counts[v] = L.quartet_counters()[1]
+            K = lists.contract_K(rl, {k: t.cpu().numpy() for k, t in mK.items()})
+            _, oK = helpers.oracle_jk_all(rl, omega=omega)
+            Ko = lists.contract_K(rl, oK)
+            assert np.abs(K - Ko).max() <= 1e-10 * max(1.0, np.abs(Ko).max()), (variant, omega)
+            assert counts[variant] == counts[1], counts
+    finally:
+        for c, v in saved.items():
+            L.set_schedule("K", c, v)

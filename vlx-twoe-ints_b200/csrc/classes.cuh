@@ -79,11 +79,19 @@ int run_coulomb_impl(const CoulombArgs& a, cudaStream_t st, Arena& ar, const Boy
     JKetPairs ket{kd.geo, kd.tmax, kd.tmin, kd.Dpp, kd.Dm, kd.Qc, kd.Dc, kd.stride, kd.n};
     int grid = launch_grid_limit();
     if ((int64_t)grid > (int64_t)a.n_ab) grid = (int)a.n_ab;
-    if (schedule_get(0, LA, LB, LC, LD) == 1)
-        coulomb_col_kernel<LA, LB, LC, LD><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut);
+    const bool col = schedule_get(0, LA, LB, LC, LD) == 1;
+    if (col)
+        coulomb_col_kernel<LA, LB, LC, LD, 0><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut);
     else
-        coulomb_kernel<LA, LB, LC, LD><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut);
+        coulomb_kernel<LA, LB, LC, LD, 0><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut);
     note_launches();
+    if (cut > 0.0) {
+        if (col)
+            coulomb_col_kernel<LA, LB, LC, LD, 1><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut);
+        else
+            coulomb_kernel<LA, LB, LC, LD, 1><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut);
+        note_launches();
+    }
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }
@@ -144,6 +152,21 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
         rc = segment_records(ar, NC * ND, npc, npd, gcd, a.pdata_cd);
         if (rc) return rc;
     }
+    const int var = schedule_get(1, LA, LB, LC, LD);
+    KGroups kgab{}, kgcd{};
+    if (var == 3 || var == 4) {
+        // contracted variants: group partner records by contracted partner shell
+        rc = contract_groups(ar, npa, gab, a.aoinds[LB], a.naos);
+        if (rc) return rc;
+        if (same) {
+            gcd = gab;
+        } else {
+            rc = contract_groups(ar, npc, gcd, a.aoinds[LD], a.naos);
+            if (rc) return rc;
+        }
+        kgab = KGroups{gab.gseg, gab.gq, gab.gbeg, gab.gcnt, gab.msp, gab.mq, gab.msu, gab.mmask};
+        kgcd = KGroups{gcd.gseg, gcd.gq, gcd.gbeg, gcd.gcnt, gcd.msp, gcd.mq, gcd.msu, gcd.mmask};
+    }
     KOutBlocks out{ko.ish, ko.ksh, ko.idx, ko.stride, ko.n};
     KPartnerRecs rab{gab.rec_sp, gab.rec_q, gab.rec_mask, gab.seg, gab.geo, gab.S, gab.sp_j, gab.sp_stride, gab.su};
     KPartnerRecs rcd{gcd.rec_sp, gcd.rec_q, gcd.rec_mask, gcd.seg, gcd.geo, gcd.S, gcd.sp_j, gcd.sp_stride, gcd.su};
@@ -152,26 +175,62 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
     unsigned long long* qc = quartet_counters_device();
     unsigned long long* qk = qc ? qc + 1 : nullptr;
     const KDensity dm{a.aoinds[LB], a.count[LB], a.aoinds[LD], a.count[LD], a.D, a.naos};
-    const int var = schedule_get(1, LA, LB, LC, LD);
-    bool launched = false;
-    if constexpr (ColTab<LA, LB, LC, LD, 0>::K_FITS) {
-        if (var == 1) {
-            exchange_col_kernel<LA, LB, LC, LD, 0><<<grid, K_THREADS, 0, st>>>(out, rab, rcd, dm, a.maxD, a.omega,
-                                                                                a.thr, a.mat_K, tab, qk, cut);
-            launched = true;
+    for (int pm = 0; pm < (cut > 0.0 ? 2 : 1); pm++) {
+        bool launched = false;
+        if constexpr (ColTab<LA, LB, LC, LD, 0>::K_FITS) {
+            if (var == 3) {
+                if (pm == 0)
+                    exchange_colc_kernel<LA, LB, LC, LD, 0, 0><<<grid, K_THREADS, 0, st>>>(
+                        out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut);
+                else
+                    exchange_colc_kernel<LA, LB, LC, LD, 0, 1><<<grid, K_THREADS, 0, st>>>(
+                        out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut);
+                launched = true;
+            }
         }
-    }
-    if constexpr (ColTab<LA, LB, LC, LD, 1>::K_FITS) {
-        if (var == 2) {
-            exchange_col_kernel<LA, LB, LC, LD, 1><<<grid, K_THREADS, 0, st>>>(out, rab, rcd, dm, a.maxD, a.omega,
-                                                                                a.thr, a.mat_K, tab, qk, cut);
-            launched = true;
+        if constexpr (ColTab<LA, LB, LC, LD, 1>::K_FITS) {
+            if (var == 4) {
+                if (pm == 0)
+                    exchange_colc_kernel<LA, LB, LC, LD, 1, 0><<<grid, K_THREADS, 0, st>>>(
+                        out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut);
+                else
+                    exchange_colc_kernel<LA, LB, LC, LD, 1, 1><<<grid, K_THREADS, 0, st>>>(
+                        out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut);
+                launched = true;
+            }
         }
+        if constexpr (ColTab<LA, LB, LC, LD, 0>::K_FITS) {
+            if (var == 1) {
+                if (pm == 0)
+                    exchange_col_kernel<LA, LB, LC, LD, 0, 0><<<grid, K_THREADS, 0, st>>>(
+                        out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut);
+                else
+                    exchange_col_kernel<LA, LB, LC, LD, 0, 1><<<grid, K_THREADS, 0, st>>>(
+                        out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut);
+                launched = true;
+            }
+        }
+        if constexpr (ColTab<LA, LB, LC, LD, 1>::K_FITS) {
+            if (var == 2) {
+                if (pm == 0)
+                    exchange_col_kernel<LA, LB, LC, LD, 1, 0><<<grid, K_THREADS, 0, st>>>(
+                        out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut);
+                else
+                    exchange_col_kernel<LA, LB, LC, LD, 1, 1><<<grid, K_THREADS, 0, st>>>(
+                        out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut);
+                launched = true;
+            }
+        }
+        if (!launched) {
+            if (pm == 0)
+                exchange_kernel<LA, LB, LC, LD, 0><<<grid, K_THREADS, 0, st>>>(out, rab, rcd, dm, a.maxD, a.omega,
+                                                                               a.thr, a.mat_K, tab, qk, cut);
+            else
+                exchange_kernel<LA, LB, LC, LD, 1><<<grid, K_THREADS, 0, st>>>(out, rab, rcd, dm, a.maxD, a.omega,
+                                                                               a.thr, a.mat_K, tab, qk, cut);
+        }
+        note_launches();
     }
-    if (!launched)
-        exchange_kernel<LA, LB, LC, LD><<<grid, K_THREADS, 0, st>>>(out, rab, rcd, dm, a.maxD, a.omega, a.thr,
-                                                                    a.mat_K, tab, qk, cut);
-    note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }

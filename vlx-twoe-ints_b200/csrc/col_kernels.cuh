@@ -70,6 +70,9 @@ struct KColShape {
     static constexpr int NL = CT::NL, P = CT::P, NXT = CT::NXT, NYT = CT::NYT;
     // phase-2 units: ori 0 -> cd pairs (accumulate K[a][c(u)]), ori 1 -> ab pairs (K[a(u)][c])
     static constexpr int N2 = ORI == 0 ? NC * ND : NA * NB;
+    // row length of the shared lane-side HRR results: odd, so that lanes
+    // storing one column of U hit distinct banks
+    static constexpr int N2P = N2 | 1;
     static constexpr int NACC = ORI == 0 ? NA : NC;
     static constexpr int NPASS = (N2 + NL - 1) / NL;
 };
@@ -78,7 +81,7 @@ template <int LA, int LB, int LC, int LD, int ORI, typename T>
 __device__ __forceinline__ void kcol_quartet(bool act, int jr, int lr, const KPartnerRecs& ab,
                                              const KPartnerRecs& cd, const KDensity& dm, double omega,
                                              const BoysTabs& tabs, const ColLane& ln, bool lane_ok, int lig,
-                                             double (*U)[KColShape<LA, LB, LC, LD, ORI>::N2],
+                                             double (*U)[KColShape<LA, LB, LC, LD, ORI>::N2P],
                                              double (*Kacc)[KColShape<LA, LB, LC, LD, ORI>::NACC])
 {
     using S = KColShape<LA, LB, LC, LD, ORI>;
@@ -192,7 +195,7 @@ __device__ __forceinline__ void kcol_quartet(bool act, int jr, int lr, const KPa
     __syncwarp();
 }
 
-template <int LA, int LB, int LC, int LD, int ORI>
+template <int LA, int LB, int LC, int LD, int ORI, int PM>
 __global__ void __launch_bounds__(K_THREADS)
 exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity dm, double maxD, double omega,
                     double thr, double* __restrict__ mat_K, BoysTabs tabs, unsigned long long* __restrict__ qcount,
@@ -204,7 +207,7 @@ exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity d
     constexpr int NW = K_THREADS / 32;
     constexpr int NL = S::NL, P = S::P, NXT = S::NXT;
     constexpr int N2 = S::N2, NACC = S::NACC, NPASS = S::NPASS;
-    __shared__ double U[NW][P][NXT][N2];
+    __shared__ double U[NW][P][NXT][S::N2P];
     __shared__ double red[NW][P][N2][NACC];
     __shared__ int s_nl[K_JCHUNK], s_n64[K_JCHUNK], s_c64[K_JCHUNK + 1], s_c32[K_JCHUNK + 1];
     const KChunk ch{s_nl, s_n64, s_c64, s_c32};
@@ -230,8 +233,8 @@ exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity d
             const int nj = min(K_JCHUNK, a1 - jb);
             k_chunk_scan(ab, cd, jb, nj, c0, c1, maxD, thr, fp32_cut, ch);
             const int t64 = s_c64[nj], t32 = s_c32[nj];
-            if (qcount && threadIdx.x == 0) atomicAdd(qcount, (unsigned long long)(t64 + t32));
-            const int n64 = (t64 + NW * P - 1) / (NW * P);
+            if (qcount && PM == 0 && threadIdx.x == 0) atomicAdd(qcount, (unsigned long long)(t64 + t32));
+            const int n64 = PM == 0 ? (t64 + NW * P - 1) / (NW * P) : 0;
             for (int it = 0; it < n64; it++) {
                 const int w = it * (NW * P) + warp * P + grp;
                 const bool act = lane_ok && w < t64;
@@ -242,7 +245,7 @@ exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity d
                 kcol_quartet<LA, LB, LC, LD, ORI, double>(act, jr, act ? lr : c0, ab, cd, dm, omega, tabs, ln,
                                                           lane_ok, lig, U[warp][gsel], Kacc);
             }
-            const int n32 = (t32 + NW * P - 1) / (NW * P);
+            const int n32 = PM == 1 ? (t32 + NW * P - 1) / (NW * P) : 0;
             for (int it = 0; it < n32; it++) {
                 const int w = it * (NW * P) + warp * P + grp;
                 const bool act = lane_ok && w < t32;
@@ -283,6 +286,251 @@ exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity d
     }
 }
 
+// ---------------------------------------------------------------- contracted exchange
+// The partner records of one first primitive shell whose partners belong to
+// one contracted shell (same centre, same AO indices) form a group.  For a
+// pair of groups (J of i, L of k) every member pair that passes the
+// reference's screen |q_j q_l max_D| > thr (gen_exchange.py:229-232) is run
+// through the VRR and its columns are summed with the weight S_ij S_kl; the
+// two HRRs and the density digestion then run once per group pair instead of
+// once per primitive quartet (Head-Gordon-Pople: the HRR coefficients AB, CD
+// do not depend on the exponents).  A record whose components do not share
+// one S is a group of its own and is digested with its per-component S.
+template <int LA, int LB, int LC, int LD, int ORI, typename T>
+__device__ __forceinline__ void col_vrr_acc(const QVT<T>& q, const T* F, const ColLane& ln, T* out, T w);
+
+struct KGroups {
+    const int* seg;          // [n_first + 1] group offsets by first primitive shell
+    const double* q;         // max member q, descending inside a segment
+    const int32_t* beg;      // first member
+    const int32_t* cnt;      // member count
+    const int32_t* msp;      // member shell pair
+    const double* mq;        // member q
+    const double* msu;       // member uniform S, or NaN (member alone in its group)
+    const uint64_t* mmask;   // member component mask
+};
+
+template <int LA, int LB, int LC, int LD, int ORI, typename T>
+__device__ __forceinline__ int kcolc_group(bool act, int jg, int lg, const KPartnerRecs& ab, const KPartnerRecs& cd,
+                                           const KGroups& gab, const KGroups& gcd, const KDensity& dm, double maxD,
+                                           double thr, double omega, const BoysTabs& tabs, const ColLane& ln,
+                                           bool lane_ok, int lig,
+                                           double (*U)[KColShape<LA, LB, LC, LD, ORI>::N2P],
+                                           double (*Kacc)[KColShape<LA, LB, LC, LD, ORI>::NACC])
+{
+    using S = KColShape<LA, LB, LC, LD, ORI>;
+    constexpr int L = LA + LB + LC + LD;
+    constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND;
+    constexpr int NL = S::NL, NXT = S::NXT, NYT = S::NYT, N2 = S::N2, NPASS = S::NPASS;
+    const int jb = act ? __ldg(gab.beg + jg) : 0, nj = act ? __ldg(gab.cnt + jg) : 0;
+    const int lb = act ? __ldg(gcd.beg + lg) : 0, nl = act ? __ldg(gcd.cnt + lg) : 0;
+    const int npair = nj * nl;
+    // every lane of the warp runs the VRR of each step (the coupling shuffles
+    // need all of them): loop to the largest member-pair count of the warp
+    int nmax = npair;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+    // a uniform side has its S folded into the sum; a non-uniform side is a
+    // single member whose per-component S is applied in the digestion
+    const bool uj = !act || !isnan(__ldg(gab.msu + jb)), ul = !act || !isnan(__ldg(gcd.msu + lb));
+    T acc[NYT];
+#pragma unroll
+    for (int y = 0; y < NYT; y++) acc[y] = (T)0;
+    int npass = 0;
+    for (int t = 0; t < nmax; t++) {
+        const bool valid = t < npair;
+        const int mj = jb + (valid ? t / nl : 0), ml = lb + (valid ? t % nl : 0);
+        const double qj = __ldg(gab.mq + mj), ql = __ldg(gcd.mq + ml);
+        const bool pass = valid && fabs(qj * ql * maxD) > thr;
+        npass += pass ? 1 : 0;
+        double w = 0.0;
+        if (pass) w = (uj ? __ldg(gab.msu + mj) : 1.0) * (ul ? __ldg(gcd.msu + ml) : 1.0);
+        const int spj = __ldg(gab.msp + mj), spl = __ldg(gcd.msp + ml);
+        const PairGeo bg = load_geo(ab.geo, ab.sp_stride, spj);
+        const PairGeo kg = load_geo(cd.geo, cd.sp_stride, spl);
+        QVT<T> q;
+        T F[L + 1];
+        make_quartet_t<L>(bg, kg, omega, tabs.f64, tabs.f32, q, F);
+        col_vrr_acc<LA, LB, LC, LD, ORI, T>(q, F, ln, acc, (T)w);
+    }
+    // HRRs and digestion once for the group pair; AB and CD from the first members
+    const int spj = __ldg(gab.msp + jb), spl = __ldg(gcd.msp + lb);
+    const T ABx = (T)__ldg(ab.geo + G_RX * ab.sp_stride + spj), ABy = (T)__ldg(ab.geo + G_RY * ab.sp_stride + spj),
+            ABz = (T)__ldg(ab.geo + G_RZ * ab.sp_stride + spj);
+    const T CDx = (T)__ldg(cd.geo + G_RX * cd.sp_stride + spl), CDy = (T)__ldg(cd.geo + G_RY * cd.sp_stride + spl),
+            CDz = (T)__ldg(cd.geo + G_RZ * cd.sp_stride + spl);
+    if (lane_ok && ln.tidx >= 0) {
+        T h[N2];
+        if (ORI == 0) hrr_bra_vector<LC, LD, T>(CDx, CDy, CDz, acc, h);
+        else hrr_bra_vector<LA, LB, T>(ABx, ABy, ABz, acc, h);
+#pragma unroll
+        for (int u = 0; u < N2; u++) U[ln.tidx][u] = (double)h[u];
+    }
+    __syncwarp();
+    if (act && npass > 0) {
+        const int jsh = __ldg(ab.partner + spj), lsh = __ldg(cd.partner + spl);
+        const uint64_t mjm = __ldg(gab.mmask + jb), mlm = __ldg(gcd.mmask + lb);
+#pragma unroll
+        for (int p = 0; p < NPASS; p++) {
+            const int u = lig + NL * p;
+            if (u < N2) {
+                T v[NXT];
+#pragma unroll
+                for (int x = 0; x < NXT; x++) v[x] = (T)U[x][u];
+                if (ORI == 0) {
+                    // unit = (c, d): bra HRR, then K[a][c] += sum_b (ab|cd) [Sij Skl] D[b][d]
+                    const int dd = u % ND;
+                    T I[NA * NB];
+                    hrr_bra_vector<LA, LB, T>(ABx, ABy, ABz, v, I);
+                    const double skl = ul ? 1.0 : (((mlm >> u) & 1ull) ? __ldg(cd.S + u * cd.sp_stride + spl) : 0.0);
+                    const uint32_t lao = __ldg(dm.d_aoinds + lsh + (int64_t)dm.d_count * dd);
+                    T wv[NB];
+#pragma unroll
+                    for (int bq = 0; bq < NB; bq++) {
+                        const uint32_t jao = __ldg(dm.b_aoinds + jsh + (int64_t)dm.b_count * bq);
+                        wv[bq] = (T)(skl * __ldg(dm.D + (int64_t)jao * dm.naos + lao));
+                    }
+#pragma unroll
+                    for (int a = 0; a < NA; a++) {
+                        T sacc = (T)0;
+#pragma unroll
+                        for (int bq = 0; bq < NB; bq++) {
+                            const T sij = uj ? (T)1 : (((mjm >> (a * NB + bq)) & 1ull)
+                                                            ? (T)__ldg(ab.S + (a * NB + bq) * ab.sp_stride + spj)
+                                                            : (T)0);
+                            sacc = fma(I[a * NB + bq] * sij, wv[bq], sacc);
+                        }
+                        Kacc[p][a] += (double)sacc;
+                    }
+                } else {
+                    // unit = (a, b): ket HRR, then K[a][c] += [Sij] sum_d (ab|cd) [Skl] D[b][d]
+                    const int bb = u % NB;
+                    T I[NC * ND];
+                    hrr_bra_vector<LC, LD, T>(CDx, CDy, CDz, v, I);
+                    const double sij = uj ? 1.0 : (((mjm >> u) & 1ull) ? __ldg(ab.S + u * ab.sp_stride + spj) : 0.0);
+                    const uint32_t jao = __ldg(dm.b_aoinds + jsh + (int64_t)dm.b_count * bb);
+                    T wv[ND];
+#pragma unroll
+                    for (int d = 0; d < ND; d++) {
+                        const uint32_t lao = __ldg(dm.d_aoinds + lsh + (int64_t)dm.d_count * d);
+                        wv[d] = (T)(sij * __ldg(dm.D + (int64_t)jao * dm.naos + lao));
+                    }
+#pragma unroll
+                    for (int c = 0; c < NC; c++) {
+                        T sacc = (T)0;
+#pragma unroll
+                        for (int d = 0; d < ND; d++) {
+                            const T skl = ul ? (T)1 : (((mlm >> (c * ND + d)) & 1ull)
+                                                           ? (T)__ldg(cd.S + (c * ND + d) * cd.sp_stride + spl)
+                                                           : (T)0);
+                            sacc = fma(I[c * ND + d] * skl, wv[d], sacc);
+                        }
+                        Kacc[p][c] += (double)sacc;
+                    }
+                }
+            }
+        }
+    }
+    __syncwarp();
+    return npass;
+}
+
+// Contracted-partner exchange kernel: exchange_col_kernel's output blocks and
+// flattened partner enumeration, over partner groups instead of records (the
+// screen on group maxima selects a superset; kcolc_group applies the exact
+// per-member screen).  PM as for coulomb_kernel, split on the group maxima.
+template <int LA, int LB, int LC, int LD, int ORI, int PM>
+__global__ void __launch_bounds__(K_THREADS, 3)
+exchange_colc_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KGroups gab, KGroups gcd, KDensity dm,
+                     double maxD, double omega, double thr, double* __restrict__ mat_K, BoysTabs tabs,
+                     unsigned long long* __restrict__ qcount, double fp32_cut)
+{
+    using S = KColShape<LA, LB, LC, LD, ORI>;
+    constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND;
+    constexpr int NAC = NA * NC;
+    constexpr int NW = K_THREADS / 32;
+    constexpr int NL = S::NL, P = S::P, NXT = S::NXT;
+    constexpr int N2 = S::N2, NACC = S::NACC, NPASS = S::NPASS;
+    __shared__ double U[NW][P][NXT][S::N2P];
+    __shared__ double red[NW][P][N2][NACC];
+    __shared__ int s_nl[K_JCHUNK], s_n64[K_JCHUNK], s_c64[K_JCHUNK + 1], s_c32[K_JCHUNK + 1];
+    const KChunk ch{s_nl, s_n64, s_c64, s_c32};
+
+    const int nout = *out.n;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane / NL, lig = lane % NL;
+    const bool lane_ok = grp < P;
+    const int gsel = lane_ok ? grp : 0;
+    const ColLane ln = make_lane<LA, LB, LC, LD, ORI>(lane_ok ? lig : 0, lane_ok ? grp * NL : lane);
+    unsigned long long nq = 0;
+
+    for (int o = blockIdx.x; o < nout; o += gridDim.x) {
+        const int ish = __ldg(out.ish + o), ksh = __ldg(out.ksh + o);
+        const int a0 = __ldg(gab.seg + ish), a1 = __ldg(gab.seg + ish + 1);
+        const int c0 = __ldg(gcd.seg + ksh), c1 = __ldg(gcd.seg + ksh + 1);
+        double Kacc[NPASS][NACC];
+#pragma unroll
+        for (int p = 0; p < NPASS; p++)
+#pragma unroll
+            for (int x = 0; x < NACC; x++) Kacc[p][x] = 0.0;
+
+        for (int jb = a0; jb < a1; jb += K_JCHUNK) {
+            const int nj = min(K_JCHUNK, a1 - jb);
+            k_chunk_scan(gab.q, gcd.q, jb, nj, c0, c1, maxD, thr, fp32_cut, ch);
+            const int t64 = s_c64[nj], t32 = s_c32[nj];
+            const int n64 = PM == 0 ? (t64 + NW * P - 1) / (NW * P) : 0;
+            for (int it = 0; it < n64; it++) {
+                const int w = it * (NW * P) + warp * P + grp;
+                const bool act = lane_ok && w < t64;
+                const int wq = act ? w : 0;
+                const int jj = k_find(s_c64, nj, wq);
+                const int np = kcolc_group<LA, LB, LC, LD, ORI, double>(
+                    act, jb + jj, c0 + (wq - s_c64[jj]), ab, cd, gab, gcd, dm, maxD, thr, omega, tabs, ln, lane_ok,
+                    lig, U[warp][gsel], Kacc);
+                if (act && lig == 0) nq += (unsigned long long)np;
+            }
+            const int n32 = PM == 1 ? (t32 + NW * P - 1) / (NW * P) : 0;
+            for (int it = 0; it < n32; it++) {
+                const int w = it * (NW * P) + warp * P + grp;
+                const bool act = lane_ok && w < t32;
+                const int wq = act ? w : 0;
+                const int jj = k_find(s_c32, nj, wq);
+                const int np = kcolc_group<LA, LB, LC, LD, ORI, float>(
+                    act, jb + jj, c0 + s_n64[jj] + (wq - s_c32[jj]), ab, cd, gab, gcd, dm, maxD, thr, omega, tabs,
+                    ln, lane_ok, lig, U[warp][gsel], Kacc);
+                if (act && lig == 0) nq += (unsigned long long)np;
+            }
+            __syncthreads();
+        }
+
+        // fixed-order reduction of the block's partials
+        if (lane_ok) {
+#pragma unroll
+            for (int p = 0; p < NPASS; p++)
+                if (lig + NL * p < N2)
+#pragma unroll
+                    for (int x = 0; x < NACC; x++) red[warp][grp][lig + NL * p][x] = Kacc[p][x];
+        }
+        __syncthreads();
+        if (threadIdx.x < NAC) {
+            const int a = threadIdx.x / NC, c = threadIdx.x % NC;
+            double sum = 0.0;
+            for (int w = 0; w < NW; w++)
+                for (int g = 0; g < P; g++) {
+                    if (ORI == 0) {
+                        for (int d = 0; d < ND; d++) sum += red[w][g][c * ND + d][a];
+                    } else {
+                        for (int b = 0; b < NB; b++) sum += red[w][g][a * NB + b][c];
+                    }
+                }
+            const int32_t pos = __ldg(out.idx + threadIdx.x * out.stride + o);
+            if (pos >= 0) mat_K[pos] += sum;
+        }
+        __syncthreads();
+    }
+    if (qcount && nq) atomicAdd(qcount, nq);
+}
+
 // ---------------------------------------------------------------- coulomb
 template <int LA, int LB, int LC, int LD, typename T>
 __device__ __forceinline__ void jcol_quartet(bool act, const PairGeo& b, double qb, const JKetPairs& ket, int kt,
@@ -307,7 +555,7 @@ __device__ __forceinline__ void jcol_quartet(bool act, const PairGeo& b, double 
     }
 }
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, int PM>
 __global__ void __launch_bounds__(J_THREADS)
 coulomb_col_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double thr, BoysTabs tabs,
                    unsigned long long* __restrict__ qcount, double fp32_cut)
@@ -336,19 +584,23 @@ coulomb_col_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, doub
             ket_prefixes(ket, nket, qb, thr, fp32_cut, ncut, nexact, n64);
             s_ncut = ncut;
             s_n64 = n64;
-            if (qcount) atomicAdd(qcount, (unsigned long long)nexact);
+            if (qcount && PM == 0) atomicAdd(qcount, (unsigned long long)nexact);
         }
         __syncthreads();
         const int ncut = s_ncut, n64 = s_n64;
+        if (PM == 1 && n64 >= ncut) {
+            __syncthreads();
+            continue;  // no FP32 quartets for this bra
+        }
         double X = 0.0;
-        const int it64 = (n64 + NW * P - 1) / (NW * P);
+        const int it64 = PM == 0 ? (n64 + NW * P - 1) / (NW * P) : 0;
         for (int it = 0; it < it64; it++) {
             const int kt0 = it * (NW * P) + warp * P + grp;
             const bool act = lane_ok && kt0 < n64;
             jcol_quartet<LA, LB, LC, LD, double>(act, b, qb, ket, act ? kt0 : 0, thr, tabs, ln, lane_ok, X);
         }
         const int n32 = ncut - n64;
-        const int it32 = (n32 + NW * P - 1) / (NW * P);
+        const int it32 = PM == 1 ? (n32 + NW * P - 1) / (NW * P) : 0;
         for (int it = 0; it < it32; it++) {
             const int kt0 = n64 + it * (NW * P) + warp * P + grp;
             const bool act = lane_ok && kt0 < ncut;

@@ -132,7 +132,20 @@ struct PairGroups {
     int* seg = nullptr;        // [npa + 1] (segmented records only)
     double* S = nullptr;       // [NXY][sp_stride] (partner records only)
     double* su = nullptr;      // [rec_stride] uniform S of a record or NaN (partner records only)
+    // contracted partner groups (contract_groups): members are the records in
+    // group order; groups sorted by descending max member q inside segments
+    int* gseg = nullptr;       // [npa + 1] group offsets by first primitive shell
+    double* gq = nullptr;      // [rec_stride] max member q
+    int32_t* gbeg = nullptr;   // [rec_stride] first member
+    int32_t* gcnt = nullptr;   // [rec_stride] member count (1..KGROUP_MAX)
+    int32_t* msp = nullptr;    // [rec_stride] member shell pair
+    double* mq = nullptr;      // [rec_stride] member q
+    double* msu = nullptr;     // [rec_stride] member uniform S or NaN (then alone in its group)
+    uint64_t* mmask = nullptr; // [rec_stride] member component mask
 };
+
+// Largest number of partner records summed before one HRR.
+constexpr int KGROUP_MAX = 8;
 
 // Group a flat list of prim-cart pairs (first[e], second[e]) by shell pair.
 int group_flat(Arena& ar, int na, int nb, int npa, int npb, const uint32_t* first, const uint32_t* second,
@@ -147,6 +160,10 @@ int make_records(Arena& ar, int nxy, PairGroups& g, const double* Q, int64_t n_e
 // Sort records by descending q inside segments of the first primitive shell,
 // and fill per-shell-pair S from the caller's pair data.
 int segment_records(Arena& ar, int nxy, int npa, int npb, PairGroups& g, const double* pdata);
+// Group segmented partner records by the partner's contracted shell (same AO
+// indices, part_aoinds = the partner type's prim_aoinds) for the contracted
+// exchange kernels.
+int contract_groups(Arena& ar, int npa, PairGroups& g, const uint32_t* part_aoinds, uint32_t naos);
 
 struct JKetData {
     double *geo, *tmax, *tmin, *Dpp, *Dm, *Qc, *Dc;

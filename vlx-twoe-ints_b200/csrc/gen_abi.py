@@ -143,7 +143,10 @@ def header():
          "/* Kernel variant used for one class (kind 0 = Coulomb: 0 one thread per",
          "   shell quartet, 1 warp-cooperative column kernel; kind 1 = exchange: 0",
          "   one thread per quartet, 1 column kernel with bra lanes, 2 column kernel",
-         "   with ket lanes).  Every variant gives the same J/K to rounding; the",
+         "   with ket lanes, 3 / 4 the column kernels with bra / ket lanes that sum",
+         "   the primitive partners of one contracted shell before the HRR).  A",
+         "   column variant whose kernel does not fit the class falls back to 0.",
+         "   Every variant gives the same J/K to rounding; the",
          "   choice only changes speed.  Set by the autotuner.  No reference",
          "   counterpart. */",
          "int vlxb_setSchedule(int kind, int la, int lb, int lc, int ld, int variant);",
@@ -155,6 +158,23 @@ def header():
          "   No reference counterpart. */",
          "int vlxb_setFp32Cutoff(double cutoff);",
          "double vlxb_getFp32Cutoff(void);", "",
+         "/* Primitive-pair -> AO contraction (the step after the class entry points,",
+         "   whose mat_J / mat_K hold one value per list entry, gen_coulomb.py:296,",
+         "   gen_exchange.py:341; the reference's caller does it on the host).",
+         "   Overwrites mat_AO (naos x naos, row-major) with the symmetric AO matrix",
+         "   M[a][b] = M[b][a] = sum of the row of (a, b), a <= b: rows r < n_rows",
+         "   with row_ao[r] = a * naos + b and entries rowptr[r] .. rowptr[r+1]-1 of",
+         "   src, each the position (bits 0..30) in pair_values of one value and a",
+         "   weight flag (bit 31: weight 2, else 1).  Summation order is the stored",
+         "   order, so results are bit-reproducible.  No reference counterpart. */",
+         "int vlxb_pairsToAO(const double* pair_values, const int64_t* rowptr, const int32_t* row_ao,",
+         "                   const uint32_t* src, int64_t n_rows, double* mat_AO, int32_t naos, void* stream);", "",
+         "/* SCF energy terms of AO matrices on the device, summed in a fixed order:",
+         "   out3[0] = Tr[D J] - Tr[D K] / 2, out3[1] = Tr[D J], out3[2] = Tr[D K]",
+         "   (device pointer; J_AO or K_AO may be NULL = zero).  No reference",
+         "   counterpart. */",
+         "int vlxb_fockEnergy(const double* D_AO, const double* J_AO, const double* K_AO, int32_t naos,",
+         "                    double* out3, void* stream);", "",
          "/* Allocation-free variant of vlxb_computeCoulombFockSSSS (same arguments,",
          "   same result) for callers that cannot allocate device memory, e.g. hosts",
          "   whose device memory is owned by their own allocator, or plugins that are",

@@ -263,7 +263,7 @@ def k_smem_bytes(plan: ColumnPlan, warps: int = 4) -> int:
     na, nb, nc, nd = ((l + 1) * (l + 2) // 2 for l in plan.cls)
     n2 = nc * nd if plan.ori == 0 else na * nb
     nacc = na if plan.ori == 0 else nc
-    U = warps * plan.P * len(plan.xtargets) * n2 * 8
+    U = warps * plan.P * len(plan.xtargets) * (n2 | 1) * 8
     red = warps * plan.P * n2 * nacc * 8
     return U + red + (256 + 1) * 4
 
@@ -272,10 +272,12 @@ def _yname(y):
     return f"{y[0]}{y[1]}{y[2]}"
 
 
-def emit_cuda(plan: ColumnPlan, T: str = "double", with_tables: bool = True):
+def emit_cuda(plan: ColumnPlan, T: str = "double", with_tables: bool = True, acc: bool = False):
     """Device function col_vrr<LA,LB,LC,LD,ORI>(q, F, ln, out): out[t] = [x|y_t]^0 for
     the lane's component x and the step-side targets y_t (plan.ytargets order).
-    Also the lane table col_tab<...> (plan.NL rows of 20 int8)."""
+    Also the lane table col_tab<...> (plan.NL rows of 20 int8).  With acc, the
+    function is col_vrr_acc(q, F, ln, out, w) and adds w * [x|y_t]^0 to out[t]
+    (primitive quartets summed before the HRR)."""
     la, lb, lc, ld = plan.cls
     ori = plan.ori
     TT = T
@@ -304,8 +306,12 @@ def emit_cuda(plan: ColumnPlan, T: str = "double", with_tables: bool = True):
         L.append(f"template <> __device__ __forceinline__ const int8_t* col_tab_ptr<{T}>() "
                  f"{{ return &col_tab_{plan.name()}[0][0]; }}")
         L.append("")
-    L.append(f"template <> __device__ __forceinline__ void col_vrr<{T}, {TT}>(const QVT<{TT}>& q, const {TT}* F, "
-             f"const ColLane& ln, {TT}* out)")
+    if acc:
+        L.append(f"template <> __device__ __forceinline__ void col_vrr_acc<{T}, {TT}>(const QVT<{TT}>& q, "
+                 f"const {TT}* F, const ColLane& ln, {TT}* out, {TT} w)")
+    else:
+        L.append(f"template <> __device__ __forceinline__ void col_vrr<{T}, {TT}>(const QVT<{TT}>& q, const {TT}* F, "
+                 f"const ColLane& ln, {TT}* out)")
     L.append("{")
     L.append(f"    const {TT} cpl = q.inv2ze;")
     L.append(f"    const {TT} cp0 = ({TT})ln.xi[0] * cpl, cp1 = ({TT})ln.xi[1] * cpl, cp2 = ({TT})ln.xi[2] * cpl;")
@@ -375,7 +381,10 @@ def emit_cuda(plan: ColumnPlan, T: str = "double", with_tables: bool = True):
         L.append(f"    const {TT} {nm} = {e};")
         cname[(y, m)] = nm
     for t, y in enumerate(plan.ytargets):
-        L.append(f"    out[{t}] = {cname[(y, 0)]};")
+        if acc:
+            L.append(f"    out[{t}] = fma(w, {cname[(y, 0)]}, out[{t}]);")
+        else:
+            L.append(f"    out[{t}] = {cname[(y, 0)]};")
     L.append("}")
     return "\n".join(L)
 
@@ -433,6 +442,10 @@ def main(outdir):
             parts.append(emit_cuda(ColumnPlan(*cls, ori), "double", True))
             parts.append("")
             parts.append(emit_cuda(ColumnPlan(*cls, ori), "float", False))
+            parts.append("")
+            parts.append(emit_cuda(ColumnPlan(*cls, ori), "double", False, acc=True))
+            parts.append("")
+            parts.append(emit_cuda(ColumnPlan(*cls, ori), "float", False, acc=True))
             parts.append("")
         parts.append("}  // namespace vlxb")
         text = "\n".join(parts) + "\n"

@@ -146,7 +146,11 @@ __device__ __forceinline__ void ket_prefixes(const JKetPairs& ket, int nket, dou
     }
 }
 
-template <int LA, int LB, int LC, int LD>
+// PM (precision pass): 0 = the FP64 quartets (every quartet when fp32_cut is
+// 0), 1 = the FP32 quartets.  The two passes are separate launches so that
+// the FP32 kernel gets its own, smaller register allocation and higher
+// occupancy; both add into mat_J, quartets are counted in pass 0.
+template <int LA, int LB, int LC, int LD, int PM>
 __global__ void __launch_bounds__(J_THREADS)
 coulomb_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double thr, BoysTabs tabs,
                unsigned long long* __restrict__ qcount, double fp32_cut)
@@ -169,18 +173,25 @@ coulomb_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double t
             ket_prefixes(ket, nket, qb, thr, fp32_cut, ncut, nexact, n64);
             s_ncut = ncut;
             s_n64 = n64;
-            if (qcount) atomicAdd(qcount, (unsigned long long)nexact);
+            if (qcount && PM == 0) atomicAdd(qcount, (unsigned long long)nexact);
         }
         __syncthreads();
         const int ncut = s_ncut, n64 = s_n64;
+        if (PM == 1 && n64 >= ncut) {
+            __syncthreads();
+            continue;  // no FP32 quartets for this bra
+        }
 
         double X[NE];
 #pragma unroll
         for (int e = 0; e < NE; e++) X[e] = 0.0;
-        for (int kt = threadIdx.x; kt < n64; kt += J_THREADS)
-            j_quartet<LA, LB, LC, LD, double>(b, qb, ket, kt, thr, tabs, X);
-        for (int kt = n64 + threadIdx.x; kt < ncut; kt += J_THREADS)
-            j_quartet<LA, LB, LC, LD, float>(b, qb, ket, kt, thr, tabs, X);
+        if (PM == 0) {
+            for (int kt = threadIdx.x; kt < n64; kt += J_THREADS)
+                j_quartet<LA, LB, LC, LD, double>(b, qb, ket, kt, thr, tabs, X);
+        } else {
+            for (int kt = n64 + threadIdx.x; kt < ncut; kt += J_THREADS)
+                j_quartet<LA, LB, LC, LD, float>(b, qb, ket, kt, thr, tabs, X);
+        }
 
 #pragma unroll
         for (int e = 0; e < NE; e++) {
@@ -251,15 +262,16 @@ struct KChunk {
     int* c32;
 };
 
-__device__ __forceinline__ void k_chunk_scan(const KPartnerRecs& ab, const KPartnerRecs& cd, int jb, int nj, int c0,
-                                             int c1, double maxD, double thr, double fp32_cut, KChunk s)
+__device__ __forceinline__ void k_chunk_scan(const double* __restrict__ aq, const double* __restrict__ cq, int jb,
+                                             int nj, int c0, int c1, double maxD, double thr, double fp32_cut,
+                                             KChunk s)
 {
     for (int t = threadIdx.x; t < nj; t += blockDim.x) {
-        const double qij = __ldg(ab.rec_q + jb + t);
+        const double qij = __ldg(aq + jb + t);
         int lo = c0, hi = c1;
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
-            if (fabs(qij * __ldg(cd.rec_q + mid) * maxD) > thr) lo = mid + 1;
+            if (fabs(qij * __ldg(cq + mid) * maxD) > thr) lo = mid + 1;
             else hi = mid;
         }
         const int nl = lo - c0;
@@ -268,7 +280,7 @@ __device__ __forceinline__ void k_chunk_scan(const KPartnerRecs& ab, const KPart
             int lo2 = c0, hi2 = lo;
             while (lo2 < hi2) {
                 const int mid = (lo2 + hi2) >> 1;
-                if (fabs(qij * __ldg(cd.rec_q + mid) * maxD) >= fp32_cut) lo2 = mid + 1;
+                if (fabs(qij * __ldg(cq + mid) * maxD) >= fp32_cut) lo2 = mid + 1;
                 else hi2 = mid;
             }
             n64 = lo2 - c0;
@@ -286,6 +298,12 @@ __device__ __forceinline__ void k_chunk_scan(const KPartnerRecs& ab, const KPart
         }
     }
     __syncthreads();
+}
+
+__device__ __forceinline__ void k_chunk_scan(const KPartnerRecs& ab, const KPartnerRecs& cd, int jb, int nj, int c0,
+                                             int c1, double maxD, double thr, double fp32_cut, KChunk s)
+{
+    k_chunk_scan(ab.rec_q, cd.rec_q, jb, nj, c0, c1, maxD, thr, fp32_cut, s);
 }
 
 // index t of the last entry with c[t] <= w (c ascending, c[0] = 0 <= w)
@@ -368,7 +386,8 @@ __device__ __forceinline__ void k_quartet(const KPartnerRecs& ab, const KPartner
         }
 }
 
-template <int LA, int LB, int LC, int LD>
+// PM as for coulomb_kernel.
+template <int LA, int LB, int LC, int LD, int PM>
 __global__ void __launch_bounds__(K_THREADS)
 exchange_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity dm, double maxD, double omega, double thr,
                 double* __restrict__ mat_K, BoysTabs tabs, unsigned long long* __restrict__ qcount, double fp32_cut)
@@ -394,15 +413,18 @@ exchange_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity dm, d
             const int nj = min(K_JCHUNK, a1 - jb);
             k_chunk_scan(ab, cd, jb, nj, c0, c1, maxD, thr, fp32_cut, ch);
             const int t64 = s_c64[nj], t32 = s_c32[nj];
-            if (qcount && threadIdx.x == 0) atomicAdd(qcount, (unsigned long long)(t64 + t32));
-            for (int w = threadIdx.x; w < t64; w += K_THREADS) {
-                const int jj = k_find(s_c64, nj, w);
-                k_quartet<LA, LB, LC, LD, double>(ab, cd, jb + jj, c0 + (w - s_c64[jj]), dm, omega, tabs, Kacc);
-            }
-            for (int w = threadIdx.x; w < t32; w += K_THREADS) {
-                const int jj = k_find(s_c32, nj, w);
-                k_quartet<LA, LB, LC, LD, float>(ab, cd, jb + jj, c0 + s_n64[jj] + (w - s_c32[jj]), dm, omega, tabs,
-                                                 Kacc);
+            if (qcount && PM == 0 && threadIdx.x == 0) atomicAdd(qcount, (unsigned long long)(t64 + t32));
+            if (PM == 0) {
+                for (int w = threadIdx.x; w < t64; w += K_THREADS) {
+                    const int jj = k_find(s_c64, nj, w);
+                    k_quartet<LA, LB, LC, LD, double>(ab, cd, jb + jj, c0 + (w - s_c64[jj]), dm, omega, tabs, Kacc);
+                }
+            } else {
+                for (int w = threadIdx.x; w < t32; w += K_THREADS) {
+                    const int jj = k_find(s_c32, nj, w);
+                    k_quartet<LA, LB, LC, LD, float>(ab, cd, jb + jj, c0 + s_n64[jj] + (w - s_c32[jj]), dm, omega,
+                                                     tabs, Kacc);
+                }
             }
             __syncthreads();
         }

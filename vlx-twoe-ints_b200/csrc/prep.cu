@@ -151,7 +151,7 @@ int schedule_set(int kind, int la, int lb, int lc, int ld, int variant)
 {
     if (kind < 0 || kind > 1 || la < 0 || la > 2 || lb < 0 || lb > 2 || lc < 0 || lc > 2 || ld < 0 || ld > 2)
         return VLXB_EINVAL;
-    if (variant < 0 || variant > (kind == 0 ? 1 : 2)) return VLXB_EINVAL;
+    if (variant < 0 || variant > (kind == 0 ? 1 : 4)) return VLXB_EINVAL;
     std::call_once(g_sched_once, sched_init);
     g_sched[kind][la * 27 + lb * 9 + lc * 3 + ld].store(variant);
     return VLXB_OK;
@@ -390,8 +390,10 @@ int segment_records(Arena& ar, int nxy, int npa, int npb, PairGroups& g, const d
         nullptr, bytes, g.rec_q, q_sorted, perm_in, perm, (int)g.rec_stride, npa, seg, seg + 1, 0, 64, st));
     void* tmp = ar.alloc<char>((int64_t)bytes);
     if (!tmp) return VLXB_ENOMEM;
-    VLXB_CHECK_CUDA(cub::DeviceSegmentedRadixSort::SortPairsDescending(
-        tmp, bytes, g.rec_q, q_sorted, perm_in, perm, (int)g.rec_stride, npa, seg, seg + 1, 0, 64, st));
+    if (!ar.measuring()) {
+        VLXB_CHECK_CUDA(cub::DeviceSegmentedRadixSort::SortPairsDescending(
+            tmp, bytes, g.rec_q, q_sorted, perm_in, perm, (int)g.rec_stride, npa, seg, seg + 1, 0, 64, st));
+    }
     if (!ar.measuring()) {
         k_gather_recs<<<prep_blocks(g.rec_stride), PREP_THREADS, 0, st>>>(g.n_rec, perm, g.rec_sp, g.rec_mask,
                                                                            sp_sorted, mask_sorted);
@@ -404,6 +406,95 @@ int segment_records(Arena& ar, int nxy, int npa, int npb, PairGroups& g, const d
     g.seg = seg;
     if (!ar.measuring()) {
         VLXB_NXY_DISPATCH(nxy, launch_sp_S, g, pdata, st);
+    }
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    return VLXB_OK;
+}
+
+struct MaxOp {
+    __device__ __forceinline__ int operator()(int a, int b) const { return a > b ? a : b; }
+};
+
+int contract_groups(Arena& ar, int npa, PairGroups& g, const uint32_t* part_aoinds, uint32_t naos)
+{
+    cudaStream_t st = ar.stream();
+    const int64_t R = g.rec_stride;
+    uint32_t* key = ar.alloc<uint32_t>(R);
+    uint32_t* key_sorted = ar.alloc<uint32_t>(R);
+    int* perm_in = ar.alloc<int>(R);
+    int* perm = ar.alloc<int>(R);
+    int* segflag = ar.alloc<int>(R + 1);
+    int* runstart = ar.alloc<int>(R);
+    int* runmax = ar.alloc<int>(R);
+    int* head = ar.alloc<int>(R + 1);
+    int* gid = ar.alloc<int>(R + 1);
+    int32_t* gbeg0 = ar.alloc<int32_t>(R);
+    double* gq0 = ar.alloc<double>(R);
+    int* gperm_in = ar.alloc<int>(R);
+    int* gperm = ar.alloc<int>(R);
+    g.gseg = ar.alloc<int>(npa + 1);
+    g.gq = ar.alloc<double>(R);
+    g.gbeg = ar.alloc<int32_t>(R);
+    g.gcnt = ar.alloc<int32_t>(R);
+    g.msp = ar.alloc<int32_t>(R);
+    g.mq = ar.alloc<double>(R);
+    g.msu = ar.alloc<double>(R);
+    g.mmask = ar.alloc<uint64_t>(R);
+    if (ar.failed()) return VLXB_ENOMEM;
+    const int nb = prep_blocks(R);
+    if (!ar.measuring()) {
+        VLXB_CHECK_CUDA(cudaMemsetAsync(segflag, 0, sizeof(int) * (R + 1), st));
+        VLXB_CHECK_CUDA(cudaMemsetAsync(head, 0, sizeof(int) * (R + 1), st));
+        k_grp_key<<<nb, PREP_THREADS, 0, st>>>(g.n_rec, g.rec_sp, g.su, g.sp_j, part_aoinds, naos, key);
+        k_iota<<<nb, PREP_THREADS, 0, st>>>(perm_in, R);
+        k_seg_starts<<<prep_blocks(npa), PREP_THREADS, 0, st>>>(g.seg, npa, segflag);
+        note_launches(3);
+    }
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    // stable key sort inside each first-shell segment (keeps descending q within a key)
+    size_t bytes = 0;
+    VLXB_CHECK_CUDA(cub::DeviceSegmentedRadixSort::SortPairs(nullptr, bytes, key, key_sorted, perm_in, perm, (int)R,
+                                                             npa, g.seg, g.seg + 1, 0, 32, st));
+    void* tmp = ar.alloc<char>((int64_t)bytes);
+    if (!tmp) return VLXB_ENOMEM;
+    if (!ar.measuring()) {
+        VLXB_CHECK_CUDA(cub::DeviceSegmentedRadixSort::SortPairs(tmp, bytes, key, key_sorted, perm_in, perm, (int)R,
+                                                                 npa, g.seg, g.seg + 1, 0, 32, st));
+        k_grp_runs<<<nb, PREP_THREADS, 0, st>>>(g.n_rec, segflag, key_sorted, runstart);
+        note_launches();
+    }
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    bytes = 0;
+    VLXB_CHECK_CUDA(cub::DeviceScan::InclusiveScan(nullptr, bytes, runstart, runmax, MaxOp(), (int)R, st));
+    tmp = ar.alloc<char>((int64_t)bytes);
+    if (!tmp) return VLXB_ENOMEM;
+    if (!ar.measuring()) {
+        VLXB_CHECK_CUDA(cub::DeviceScan::InclusiveScan(tmp, bytes, runstart, runmax, MaxOp(), (int)R, st));
+        k_grp_heads<<<nb, PREP_THREADS, 0, st>>>(g.n_rec, runmax, KGROUP_MAX, head);
+        note_launches();
+    }
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    int rc = scan_int(ar, head, gid, R + 1);
+    if (rc) return rc;
+    if (!ar.measuring()) {
+        k_grp_fill<<<nb, PREP_THREADS, 0, st>>>(g.n_rec, perm, head, gid, g.rec_sp, g.rec_q, g.su, g.rec_mask, g.msp,
+                                                g.mq, g.msu, g.mmask, gbeg0, gq0);
+        k_grp_seg<<<prep_blocks(npa + 1), PREP_THREADS, 0, st>>>(g.seg, npa, gid, g.gseg);
+        k_iota<<<nb, PREP_THREADS, 0, st>>>(gperm_in, R);
+        note_launches(3);
+    }
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    // groups by descending max q inside each segment
+    bytes = 0;
+    VLXB_CHECK_CUDA(cub::DeviceSegmentedRadixSort::SortPairsDescending(nullptr, bytes, gq0, g.gq, gperm_in, gperm,
+                                                                       (int)R, npa, g.gseg, g.gseg + 1, 0, 64, st));
+    tmp = ar.alloc<char>((int64_t)bytes);
+    if (!tmp) return VLXB_ENOMEM;
+    if (!ar.measuring()) {
+        VLXB_CHECK_CUDA(cub::DeviceSegmentedRadixSort::SortPairsDescending(
+            tmp, bytes, gq0, g.gq, gperm_in, gperm, (int)R, npa, g.gseg, g.gseg + 1, 0, 64, st));
+        k_grp_order<<<nb, PREP_THREADS, 0, st>>>(g.gseg + npa, g.n_rec, gperm, gbeg0, g.gbeg, g.gcnt);
+        note_launches();
     }
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;

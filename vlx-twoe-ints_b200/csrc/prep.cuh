@@ -321,4 +321,93 @@ __global__ void k_kout_fill(const uint32_t* __restrict__ pi, const uint32_t* __r
     }
 }
 
+// ------------------------------------------------------------ contracted partner groups
+// Partner records of one first primitive shell whose partners belong to one
+// contracted shell share the partner's centre and AO indices, so their
+// primitive quartets can be summed before the HRR (Head-Gordon-Pople).  A
+// record is groupable when one S covers all its components (su not NaN); its
+// key is then the AO index of the partner's first component.  Other records
+// get a key of their own (naos + r) and stay alone.
+__global__ void k_grp_key(const int* __restrict__ n_rec, const int32_t* __restrict__ rec_sp,
+                          const double* __restrict__ su, const int32_t* __restrict__ sp_j,
+                          const uint32_t* __restrict__ part_aoinds, uint32_t naos, uint32_t* __restrict__ key)
+{
+    const int n = *n_rec;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+        key[r] = isnan(su[r]) ? naos + (uint32_t)r : part_aoinds[sp_j[rec_sp[r]]];
+}
+
+// flag[seg[i]] = 1 for every non-empty segment i (flag zeroed by the caller)
+__global__ void k_seg_starts(const int* __restrict__ seg, int nseg, int* __restrict__ flag)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nseg; i += gridDim.x * blockDim.x)
+        if (seg[i] < seg[i + 1]) flag[seg[i]] = 1;
+}
+
+// After the key sort: a run starts at a segment start or where the key changes;
+// runstart[r] = r at run starts, 0 elsewhere (max-scanned by the caller).
+__global__ void k_grp_runs(const int* __restrict__ n_rec, const int* __restrict__ segflag,
+                           const uint32_t* __restrict__ key_sorted, int* __restrict__ runstart)
+{
+    const int n = *n_rec;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+        runstart[r] = (r == 0 || segflag[r] || key_sorted[r] != key_sorted[r - 1]) ? r : 0;
+}
+
+// Group heads: run starts, and every MAXG-th record of a run (groups hold at
+// most MAXG members).  head[r] for r >= n_rec stays 0.
+__global__ void k_grp_heads(const int* __restrict__ n_rec, const int* __restrict__ runmax, int maxg,
+                            int* __restrict__ head)
+{
+    const int n = *n_rec;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+        head[r] = ((r - runmax[r]) % maxg) == 0 ? 1 : 0;
+}
+
+// Members in key order (gathered through the sort permutation) and one entry
+// per group: first member, member count, max member q (the first member's:
+// the key sort is stable and records arrive sorted by descending q).
+__global__ void k_grp_fill(const int* __restrict__ n_rec, const int* __restrict__ perm,
+                           const int* __restrict__ head, const int* __restrict__ gid,
+                           const int32_t* __restrict__ rec_sp, const double* __restrict__ rec_q,
+                           const double* __restrict__ su, const uint64_t* __restrict__ rec_mask,
+                           int32_t* __restrict__ msp, double* __restrict__ mq, double* __restrict__ msu,
+                           uint64_t* __restrict__ mmask, int32_t* __restrict__ gbeg, double* __restrict__ gq)
+{
+    const int n = *n_rec;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const int p = perm[r];
+        msp[r] = rec_sp[p];
+        mq[r] = rec_q[p];
+        msu[r] = su[p];
+        mmask[r] = rec_mask[p];
+        if (head[r]) {
+            gbeg[gid[r]] = r;
+            gq[gid[r]] = rec_q[p];
+        }
+    }
+}
+
+// Group segment offsets gseg[i] = gid[seg[i]] (gid exclusive scan of heads,
+// n_rec + 1 entries), member counts from consecutive group starts.
+__global__ void k_grp_seg(const int* __restrict__ seg, int nseg, const int* __restrict__ gid,
+                          int* __restrict__ gseg)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= nseg; i += gridDim.x * blockDim.x)
+        gseg[i] = gid[seg[i]];
+}
+
+__global__ void k_grp_order(const int* __restrict__ n_grp, const int* __restrict__ n_rec,
+                            const int* __restrict__ gperm, const int32_t* __restrict__ gbeg_in,
+                            int32_t* __restrict__ gbeg, int32_t* __restrict__ gcnt)
+{
+    const int n = *n_grp, nr = *n_rec;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const int g = gperm[t];
+        const int b = gbeg_in[g];
+        gbeg[t] = b;
+        gcnt[t] = (g + 1 < n ? gbeg_in[g + 1] : nr) - b;
+    }
+}
+
 }  // namespace vlxb

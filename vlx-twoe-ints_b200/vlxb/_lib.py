@@ -77,6 +77,10 @@ class Lib:
         c.vlxb_fp64Probe.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         c.vlxb_setFp32Cutoff.argtypes = [ctypes.c_double]
         c.vlxb_getFp32Cutoff.restype = ctypes.c_double
+        c.vlxb_pairsToAO.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_int64, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]
+        c.vlxb_fockEnergy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                      ctypes.c_void_p, ctypes.c_void_p]
 
     def check(self, rc: int, what: str):
         if rc != 0:
@@ -121,6 +125,16 @@ class Lib:
         out = ctypes.c_ulonglong(0)
         self.check(self.cdll.vlxb_launchCount(ctypes.byref(out), int(reset)), "vlxb_launchCount")
         return int(out.value)
+
+    def pairs_to_ao(self, values: int, rowptr: int, row_ao: int, src: int, n_rows: int, out: int, naos: int,
+                    stream: int = 0):
+        """vlxb_pairsToAO on raw device pointers (see include/vlxb.h)."""
+        self.check(self.cdll.vlxb_pairsToAO(values, rowptr, row_ao, src, int(n_rows), out, int(naos), stream),
+                   "vlxb_pairsToAO")
+
+    def fock_energy(self, D: int, J: int, K: int, naos: int, out3: int, stream: int = 0):
+        """vlxb_fockEnergy on raw device pointers (J or K may be 0 = NULL)."""
+        self.check(self.cdll.vlxb_fockEnergy(D, J or None, K or None, int(naos), out3, stream), "vlxb_fockEnergy")
 
     def reset_counters(self, stream: int = 0):
         self.check(self.cdll.vlxb_quartetCounters(None, 1, stream), "vlxb_quartetCounters")

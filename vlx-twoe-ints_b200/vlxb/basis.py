@@ -194,3 +194,27 @@ def config_custom(natoms: int, side: float, recipe: dict, degree: int, alpha0: f
     mol = build_molecule(coords, recipe, degree=degree, alpha0=alpha0, ratio=ratio, rng=rng)
     D = make_density(mol, nocc, np.random.default_rng(seed + 1))
     return Workload(f"{natoms} atoms custom", mol, D, threshold, nocc)
+
+
+def molecule_at_density(natoms: int, bohr3_per_atom: float, seed: int, threshold: float = 1e-12) -> Workload:
+    """One molecule of the batched / served workloads: `natoms` atoms placed in a
+    cube of side (natoms * bohr3_per_atom)^(1/3) bohr, the 4s+3p+2d recipe of
+    degree 3 (alpha = 0.05 * 2.5^k), 2 occupied orbitals per atom."""
+    side = (natoms * bohr3_per_atom) ** (1.0 / 3.0)
+    wl = config_custom(natoms, side, {0: 4, 1: 3, 2: 2}, 3, 0.05, 2.5, 2 * natoms, threshold, seed)
+    wl.name = f"{natoms} atoms 4s3p2d at {bohr3_per_atom:g} bohr^3/atom"
+    return wl
+
+
+def config_batch(n_mols: int = 256, atoms=(3, 30), bohr3_per_atom: float = 30.0, seed: int = 0) -> list:
+    """Batched workload: n_mols independent molecules, atom counts uniform in
+    [atoms[0], atoms[1]], 1 atom per 30 bohr^3, the 4s+3p+2d recipe."""
+    rng = np.random.default_rng(seed)
+    counts = rng.integers(atoms[0], atoms[1] + 1, size=n_mols)
+    return [molecule_at_density(int(n), bohr3_per_atom, seed * 100003 + t) for t, n in enumerate(counts)]
+
+
+def serve_atom_counts(n_req: int, lo: int = 5, hi: int = 120, seed: int = 0) -> np.ndarray:
+    """Atom counts of served requests: log-uniform on [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    return np.exp(rng.uniform(np.log(lo), np.log(hi + 1), size=n_req)).astype(int).clip(lo, hi)

@@ -42,7 +42,7 @@ def compiled_variants(kind: str, cls: str):
     out = [] if cls in SPILLING_THREAD_KERNELS["K"] else [0]
     for ori in (0, 1):
         if k_smem_bytes(ColumnPlan(*l, ori)) <= 46 * 1024:
-            out.append(1 + ori)
+            out += [1 + ori, 3 + ori]
     return out
 
 
