@@ -36,3 +36,21 @@ def test_map_equals_host_contraction():
 def test_empty_map():
     rowptr, row_ao, src = aomap.build_map(7, [])
     assert rowptr.tolist() == [0] and len(row_ao) == 0 and len(src) == 0
+
+
+def test_torch_map_equals_numpy_map():
+    """AOMap.from_device (torch ops; run here on CPU tensors) builds exactly
+    the numpy map of AOMap(rl)."""
+    import torch
+    from vlxb import fock
+
+    mol, D = tiny_molecule(seed=9)
+    rl = lists.build_lists(mol, D, 1e-12, helpers.oracle_schwarz_fn)
+    ref = aomap.AOMap(rl, device="cpu")
+    dl = fock.to_device(rl, "cpu")
+    got = aomap.AOMap.from_device(dl)
+    for a, b in ((ref.J, got.J), (ref.K, got.K)):
+        assert a.keys == b.keys and a.sizes == b.sizes
+        assert torch.equal(a.rowptr, b.rowptr)
+        assert torch.equal(a.row_ao, b.row_ao)
+        assert torch.equal(a.src, b.src)

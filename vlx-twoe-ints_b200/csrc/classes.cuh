@@ -23,6 +23,12 @@ struct CoulombArgs {
     const double* cd_pdata;
     uint32_t n_cd;
     double thr;
+    // batched calls over several molecules (null / 0 for a class call): the
+    // molecule of every primitive of types a and c; a bra pairs only with
+    // kets of its own molecule
+    const int32_t* prim_mol_a;
+    const int32_t* prim_mol_c;
+    int n_mol;
 };
 
 struct ExchangeArgs {
@@ -43,6 +49,12 @@ struct ExchangeArgs {
     const double *pdata_ab, *pdata_cd;
     double omega;
     double thr;
+    // batched calls over several molecules (all null / 0 for a class call):
+    const uint32_t* aoinds_col[3];  // density column index per prim component (default: aoinds)
+    uint32_t D_stride;              // row stride of D (default: naos)
+    uint32_t key_naos;              // bound on the AO indices in aoinds (default: naos)
+    const int32_t* prim_mol_a;      // molecule of every type-a primitive
+    const double* maxD_mol;         // [molecules] max |D| bound of each molecule
 };
 
 // Coulomb class call on a given arena (pool, static or measuring) with given
@@ -70,13 +82,20 @@ int run_coulomb_impl(const CoulombArgs& a, cudaStream_t st, Arena& ar, const Boy
     rc = group_flat(ar, NC, ND, (int)a.count[LC], (int)a.count[LD], a.cd_first, a.cd_second, a.n_cd, a.info[LC],
                     a.count[LC], a.info[LD], a.count[LD], gk);
     if (rc) return rc;
+    const bool batched = a.prim_mol_a && a.prim_mol_c && a.n_mol > 0;
     JKetData kd;
-    rc = jket_prepare<LC, LD>(ar, gk, a.cd_first, a.cd_second, a.cd_D, a.cd_Q, a.cd_pdata, kd);
+    rc = jket_prepare<LC, LD>(ar, gk, a.cd_first, a.cd_second, a.cd_D, a.cd_Q, a.cd_pdata, kd,
+                              batched ? a.prim_mol_c : nullptr, batched ? a.n_mol : 0);
     if (rc) return rc;
+    int32_t* bmol = nullptr;
+    if (batched) {
+        rc = bra_record_mol(ar, gb, a.prim_mol_a, &bmol);
+        if (rc) return rc;
+    }
     if (ar.failed()) return VLXB_ENOMEM;
     if (ar.measuring()) return VLXB_OK;
-    JBraRecs bra{gb.rec_sp, gb.rec_q, gb.rec_mask, gb.n_rec, gb.geo, gb.entry, gb.sp_stride, a.ab_pdata};
-    JKetPairs ket{kd.geo, kd.tmax, kd.tmin, kd.Dpp, kd.Dm, kd.Qc, kd.Dc, kd.stride, kd.n};
+    JBraRecs bra{gb.rec_sp, gb.rec_q, gb.rec_mask, gb.n_rec, gb.geo, gb.entry, gb.sp_stride, a.ab_pdata, bmol};
+    JKetPairs ket{kd.geo, kd.tmax, kd.tmin, kd.Dpp, kd.Dm, kd.Qc, kd.Dc, kd.stride, kd.n, batched ? kd.seg : nullptr};
     int grid = launch_grid_limit();
     if ((int64_t)grid > (int64_t)a.n_ab) grid = (int)a.n_ab;
     const bool col = schedule_get(0, LA, LB, LC, LD) == 1;
@@ -154,27 +173,34 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
     }
     const int var = schedule_get(1, LA, LB, LC, LD);
     KGroups kgab{}, kgcd{};
+    const uint32_t key_naos = a.key_naos ? a.key_naos : a.naos;
     if (var == 3 || var == 4) {
         // contracted variants: group partner records by contracted partner shell
-        rc = contract_groups(ar, npa, gab, a.aoinds[LB], a.naos);
+        rc = contract_groups(ar, npa, gab, a.aoinds[LB], key_naos);
         if (rc) return rc;
         if (same) {
             gcd = gab;
         } else {
-            rc = contract_groups(ar, npc, gcd, a.aoinds[LD], a.naos);
+            rc = contract_groups(ar, npc, gcd, a.aoinds[LD], key_naos);
             if (rc) return rc;
         }
         kgab = KGroups{gab.gseg, gab.gq, gab.gbeg, gab.gcnt, gab.msp, gab.mq, gab.msu, gab.mmask};
         kgcd = KGroups{gcd.gseg, gcd.gq, gcd.gbeg, gcd.gcnt, gcd.msp, gcd.mq, gcd.msu, gcd.mmask};
     }
-    KOutBlocks out{ko.ish, ko.ksh, ko.idx, ko.stride, ko.n};
+    double* blk_maxD = nullptr;
+    if (a.prim_mol_a && a.maxD_mol) {
+        rc = kout_block_maxd(ar, ko, a.prim_mol_a, a.maxD_mol, &blk_maxD);
+        if (rc) return rc;
+    }
+    KOutBlocks out{ko.ish, ko.ksh, ko.idx, ko.stride, ko.n, blk_maxD};
     KPartnerRecs rab{gab.rec_sp, gab.rec_q, gab.rec_mask, gab.seg, gab.geo, gab.S, gab.sp_j, gab.sp_stride, gab.su};
     KPartnerRecs rcd{gcd.rec_sp, gcd.rec_q, gcd.rec_mask, gcd.seg, gcd.geo, gcd.S, gcd.sp_j, gcd.sp_stride, gcd.su};
     int grid = launch_grid_limit();
     if ((int64_t)grid > (int64_t)a.n_ik) grid = (int)a.n_ik;
     unsigned long long* qc = quartet_counters_device();
     unsigned long long* qk = qc ? qc + 1 : nullptr;
-    const KDensity dm{a.aoinds[LB], a.count[LB], a.aoinds[LD], a.count[LD], a.D, a.naos};
+    const KDensity dm{a.aoinds[LB], a.count[LB], a.aoinds_col[LD] ? a.aoinds_col[LD] : a.aoinds[LD], a.count[LD],
+                      a.D, a.D_stride ? a.D_stride : a.naos};
     for (int pm = 0; pm < (cut > 0.0 ? 2 : 1); pm++) {
         bool launched = false;
         if constexpr (ColTab<LA, LB, LC, LD, 0>::K_FITS) {

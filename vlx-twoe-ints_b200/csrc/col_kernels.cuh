@@ -221,6 +221,7 @@ exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity d
 
     for (int o = blockIdx.x; o < nout; o += gridDim.x) {
         const int ish = __ldg(out.ish + o), ksh = __ldg(out.ksh + o);
+        const double mD = out.maxD ? __ldg(out.maxD + o) : maxD;
         const int a0 = __ldg(ab.seg + ish), a1 = __ldg(ab.seg + ish + 1);
         const int c0 = __ldg(cd.seg + ksh), c1 = __ldg(cd.seg + ksh + 1);
         double Kacc[NPASS][NACC];
@@ -231,7 +232,7 @@ exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity d
 
         for (int jb = a0; jb < a1; jb += K_JCHUNK) {
             const int nj = min(K_JCHUNK, a1 - jb);
-            k_chunk_scan(ab, cd, jb, nj, c0, c1, maxD, thr, fp32_cut, ch);
+            k_chunk_scan(ab, cd, jb, nj, c0, c1, mD, thr, fp32_cut, ch);
             const int t64 = s_c64[nj], t32 = s_c32[nj];
             if (qcount && PM == 0 && threadIdx.x == 0) atomicAdd(qcount, (unsigned long long)(t64 + t32));
             const int n64 = PM == 0 ? (t64 + NW * P - 1) / (NW * P) : 0;
@@ -439,6 +440,8 @@ __device__ __forceinline__ int kcolc_group(bool act, int jg, int lg, const KPart
 // flattened partner enumeration, over partner groups instead of records (the
 // screen on group maxima selects a superset; kcolc_group applies the exact
 // per-member screen).  PM as for coulomb_kernel, split on the group maxima.
+// Registers are capped for 3 CTAs per SM (168): the heaviest classes spill a
+// little; a 2-CTA cap (no spills, fewer warps) measured no faster.
 template <int LA, int LB, int LC, int LD, int ORI, int PM>
 __global__ void __launch_bounds__(K_THREADS, 3)
 exchange_colc_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KGroups gab, KGroups gcd, KDensity dm,
@@ -466,6 +469,7 @@ exchange_colc_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KGroups g
 
     for (int o = blockIdx.x; o < nout; o += gridDim.x) {
         const int ish = __ldg(out.ish + o), ksh = __ldg(out.ksh + o);
+        const double mD = out.maxD ? __ldg(out.maxD + o) : maxD;
         const int a0 = __ldg(gab.seg + ish), a1 = __ldg(gab.seg + ish + 1);
         const int c0 = __ldg(gcd.seg + ksh), c1 = __ldg(gcd.seg + ksh + 1);
         double Kacc[NPASS][NACC];
@@ -476,7 +480,7 @@ exchange_colc_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KGroups g
 
         for (int jb = a0; jb < a1; jb += K_JCHUNK) {
             const int nj = min(K_JCHUNK, a1 - jb);
-            k_chunk_scan(gab.q, gcd.q, jb, nj, c0, c1, maxD, thr, fp32_cut, ch);
+            k_chunk_scan(gab.q, gcd.q, jb, nj, c0, c1, mD, thr, fp32_cut, ch);
             const int t64 = s_c64[nj], t32 = s_c32[nj];
             const int n64 = PM == 0 ? (t64 + NW * P - 1) / (NW * P) : 0;
             for (int it = 0; it < n64; it++) {
@@ -485,7 +489,7 @@ exchange_colc_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KGroups g
                 const int wq = act ? w : 0;
                 const int jj = k_find(s_c64, nj, wq);
                 const int np = kcolc_group<LA, LB, LC, LD, ORI, double>(
-                    act, jb + jj, c0 + (wq - s_c64[jj]), ab, cd, gab, gcd, dm, maxD, thr, omega, tabs, ln, lane_ok,
+                    act, jb + jj, c0 + (wq - s_c64[jj]), ab, cd, gab, gcd, dm, mD, thr, omega, tabs, ln, lane_ok,
                     lig, U[warp][gsel], Kacc);
                 if (act && lig == 0) nq += (unsigned long long)np;
             }
@@ -496,7 +500,7 @@ exchange_colc_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KGroups g
                 const int wq = act ? w : 0;
                 const int jj = k_find(s_c32, nj, wq);
                 const int np = kcolc_group<LA, LB, LC, LD, ORI, float>(
-                    act, jb + jj, c0 + s_n64[jj] + (wq - s_c32[jj]), ab, cd, gab, gcd, dm, maxD, thr, omega, tabs,
+                    act, jb + jj, c0 + s_n64[jj] + (wq - s_c32[jj]), ab, cd, gab, gcd, dm, mD, thr, omega, tabs,
                     ln, lane_ok, lig, U[warp][gsel], Kacc);
                 if (act && lig == 0) nq += (unsigned long long)np;
             }
@@ -579,12 +583,18 @@ coulomb_col_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, doub
         const int sp = __ldg(bra.rec_sp + r);
         const PairGeo b = load_geo(bra.geo, bra.sp_stride, sp);
         const double qb = __ldg(bra.rec_q + r);
+        int k0 = 0, k1 = nket;
+        if (bra.mol) {
+            const int m = __ldg(bra.mol + r);
+            k0 = __ldg(ket.seg + m);
+            k1 = __ldg(ket.seg + m + 1);
+        }
         if (threadIdx.x == 0) {
             int ncut, nexact, n64;
-            ket_prefixes(ket, nket, qb, thr, fp32_cut, ncut, nexact, n64);
+            ket_prefixes(ket, k0, k1, qb, thr, fp32_cut, ncut, nexact, n64);
             s_ncut = ncut;
             s_n64 = n64;
-            if (qcount && PM == 0) atomicAdd(qcount, (unsigned long long)nexact);
+            if (qcount && PM == 0) atomicAdd(qcount, (unsigned long long)(nexact - k0));
         }
         __syncthreads();
         const int ncut = s_ncut, n64 = s_n64;
@@ -593,9 +603,9 @@ coulomb_col_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, doub
             continue;  // no FP32 quartets for this bra
         }
         double X = 0.0;
-        const int it64 = PM == 0 ? (n64 + NW * P - 1) / (NW * P) : 0;
+        const int it64 = PM == 0 ? (n64 - k0 + NW * P - 1) / (NW * P) : 0;
         for (int it = 0; it < it64; it++) {
-            const int kt0 = it * (NW * P) + warp * P + grp;
+            const int kt0 = k0 + it * (NW * P) + warp * P + grp;
             const bool act = lane_ok && kt0 < n64;
             jcol_quartet<LA, LB, LC, LD, double>(act, b, qb, ket, act ? kt0 : 0, thr, tabs, ln, lane_ok, X);
         }

@@ -169,10 +169,16 @@ struct JKetData {
     double *geo, *tmax, *tmin, *Dpp, *Dm, *Qc, *Dc;
     int64_t stride;
     int* n;
+    int* seg = nullptr;  // [n_mol + 1] ket offsets per molecule (batched calls)
 };
+// prim_mol_c (batched calls, else null): molecule of every type-c primitive;
+// the kets are then sorted by molecule, and by descending bound inside one.
 template <int LC, int LD>
 int jket_prepare(Arena& ar, const PairGroups& g, const uint32_t* first, const uint32_t* second,
-                 const double* D, const double* Q, const double* pdata, JKetData& out);
+                 const double* D, const double* Q, const double* pdata, JKetData& out,
+                 const int32_t* prim_mol_c = nullptr, int n_mol = 0);
+// Molecule of every bra record (batched Coulomb calls).
+int bra_record_mol(Arena& ar, const PairGroups& g, const int32_t* prim_mol_a, int32_t** mol);
 
 struct KOutData {
     int32_t *ish, *ksh, *idx;
@@ -181,6 +187,9 @@ struct KOutData {
 };
 int kout_prepare(Arena& ar, int na, int nc, int npa, int npc, const uint32_t* pi, const uint32_t* pk, int64_t n,
                  KOutData& out);
+// Per-block max |D| of a batched exchange call (molecule of the block's i).
+int kout_block_maxd(Arena& ar, const KOutData& ko, const int32_t* prim_mol_a, const double* maxD_mol,
+                    double** out);
 
 int launch_grid_limit();
 

@@ -175,6 +175,64 @@ def header():
          "   counterpart. */",
          "int vlxb_fockEnergy(const double* D_AO, const double* J_AO, const double* K_AO, int32_t naos,",
          "                    double* out3, void* stream);", "",
+         "/* Caller-side list inputs on the device (the reference's caller computes",
+         "   them outside the generator: pair data, Q, cd_mat_D and bd_max_D of",
+         "   gen_coulomb.py:80-90 and gen_exchange.py:78-110).  No reference",
+         "   counterpart.",
+         "   vlxb_shellPairData: for n primitive shell pairs (P[t] of type la, Q[t]",
+         "   of type lb, la <= lb <= 2) S_out[t] = c_P c_Q (pi/p)^(3/2)",
+         "   exp(-ab/p |A-B|^2) and q_out[t] = |S_out[t]| * max over components",
+         "   sqrt|(ab|ab)| / |S_ab| (the Schwarz value of every component pair).",
+         "   vlxb_gatherPairDensity: out[t] = D_AO[ao_a(first[t])][ao_b(second[t])]",
+         "   with ao_x(i) = aoinds_x[(i % ncart_x) * cnt_x + i / ncart_x].",
+         "   vlxb_blockMaxAbs: *out (device) = max |D_AO[r][c]|, r in rows[0..nrows),",
+         "   c in cols[0..ncols). */",
+         "int vlxb_shellPairData(int la, int lb, const double* info_a, uint32_t cnt_a, const double* info_b,",
+         "                       uint32_t cnt_b, const uint32_t* P, const uint32_t* Q, uint32_t n, double* S_out,",
+         "                       double* q_out, void* stream);",
+         "int vlxb_gatherPairDensity(const double* D_AO, uint32_t naos, const uint32_t* first, const uint32_t* second,",
+         "                           const uint32_t* aoinds_a, int ncart_a, uint32_t cnt_a, const uint32_t* aoinds_b,",
+         "                           int ncart_b, uint32_t cnt_b, int64_t n, double* out, void* stream);",
+         "int vlxb_blockMaxAbs(const double* D_AO, uint32_t naos, const uint32_t* rows, int64_t nrows,",
+         "                     const uint32_t* cols, int64_t ncols, double* out, void* stream);", "",
+         "/* Batched class calls: one call of class (la lb|lc ld) covers many",
+         "   independent molecules whose lists are concatenated (the union of their",
+         "   primitives per type, no pair across two molecules).  No reference",
+         "   counterpart (the reference ABI carries no molecule boundaries).",
+         "   Coulomb: a bra pairs only with kets of its own molecule (prim_mol[la],",
+         "   prim_mol[lc]); the lists are the reference's J lists of the union, the",
+         "   result per molecule is the class call of that molecule alone.",
+         "   Exchange: the reference's K lists of the union; the density is read as",
+         "   D[row][col] with row = prim_aoinds (AO index in the union), col =",
+         "   prim_aocols (column in a stack of per-molecule density blocks of row",
+         "   stride D_stride), and each output block is screened with its own",
+         "   molecule's bound maxD_mol[prim_mol[la][i]].  Unused fields: 0 / NULL. */",
+         "typedef struct {",
+         "    double* mat;                      /* mat_J or mat_K (accumulated with +=) */",
+         "    const double* prim_info[3];       /* union prim_info of s, p, d */",
+         "    const uint32_t* prim_aoinds[3];   /* AO index per component (union numbering) */",
+         "    const uint32_t* prim_aocols[3];   /* exchange: density column per component */",
+         "    uint32_t prim_count[3];",
+         "    const int32_t* prim_mol[3];       /* molecule of every primitive */",
+         "    int32_t n_mol;",
+         "    /* Coulomb (gen_coulomb.py:80-90 arguments of the union) */",
+         "    const double *ab_Q, *cd_Q, *cd_D, *ab_pdata, *cd_pdata;",
+         "    const uint32_t *ab_first, *ab_second, *cd_first, *cd_second;",
+         "    uint32_t n_ab, n_cd;",
+         "    /* Exchange (gen_exchange.py:78-110 arguments of the union) */",
+         "    const uint32_t *pair_i, *pair_k;",
+         "    uint32_t n_ik;",
+         "    const double* D;",
+         "    uint32_t D_stride;                /* row stride of D */",
+         "    uint32_t naos;                    /* AOs of the union (bound on prim_aoinds) */",
+         "    const double* maxD_mol;           /* [n_mol] max |D| of each molecule's bd block */",
+         "    const double *Q_ab, *Q_cd, *pdata_ab, *pdata_cd;",
+         "    const uint32_t *Dinds_ab, *Dinds_cd, *displs_ab, *displs_cd, *counts_ab, *counts_cd;",
+         "    double omega;",
+         "    double thr;",
+         "} VlxbBatchCall;",
+         "int vlxb_coulombBatch(int la, int lb, int lc, int ld, const VlxbBatchCall* call, void* stream);",
+         "int vlxb_exchangeBatch(int la, int lb, int lc, int ld, const VlxbBatchCall* call, void* stream);", "",
          "/* Allocation-free variant of vlxb_computeCoulombFockSSSS (same arguments,",
          "   same result) for callers that cannot allocate device memory, e.g. hosts",
          "   whose device memory is owned by their own allocator, or plugins that are",
@@ -255,6 +313,43 @@ def abi_cu():
         L.append("    A.omega = omega; A.thr = eri_threshold;")
         L.append(f"    return vlxb::exchange_{cls}(A, (cudaStream_t)stream);")
         L += ["}", ""]
+    # batched calls: runtime class -> the class units
+    L += ["int vlxb_coulombBatch(int la, int lb, int lc, int ld, const VlxbBatchCall* c, void* stream)", "{",
+          "    if (la < 0 || la > 2 || lb < 0 || lb > 2 || lc < 0 || lc > 2 || ld < 0 || ld > 2) return VLXB_EINVAL;",
+          "    if (!c || c->n_mol <= 0 || !c->prim_mol[la] || !c->prim_mol[lc]) return VLXB_EINVAL;",
+          "    vlxb::CoulombArgs A{};",
+          "    A.mat_J = c->mat;",
+          "    for (int l = 0; l < 3; l++) { A.info[l] = c->prim_info[l]; A.count[l] = c->prim_count[l]; }",
+          "    A.cd_D = c->cd_D; A.ab_Q = c->ab_Q; A.cd_Q = c->cd_Q;",
+          "    A.ab_first = c->ab_first; A.ab_second = c->ab_second; A.ab_pdata = c->ab_pdata; A.n_ab = c->n_ab;",
+          "    A.cd_first = c->cd_first; A.cd_second = c->cd_second; A.cd_pdata = c->cd_pdata; A.n_cd = c->n_cd;",
+          "    A.thr = c->thr;",
+          "    A.prim_mol_a = c->prim_mol[la]; A.prim_mol_c = c->prim_mol[lc]; A.n_mol = c->n_mol;",
+          "    switch (la * 27 + lb * 9 + lc * 3 + ld) {"]
+    for cls in j_classes():
+        la, lb, lc, ld = (LV[x] for x in cls)
+        L.append(f"        case {la * 27 + lb * 9 + lc * 3 + ld}: return vlxb::coulomb_{cls}(A, (cudaStream_t)stream);")
+    L += ["        default: return VLXB_EINVAL;", "    }", "}", ""]
+    L += ["int vlxb_exchangeBatch(int la, int lb, int lc, int ld, const VlxbBatchCall* c, void* stream)", "{",
+          "    if (la < 0 || la > 2 || lb < 0 || lb > 2 || lc < 0 || lc > 2 || ld < 0 || ld > 2) return VLXB_EINVAL;",
+          "    if (!c || c->n_mol <= 0 || !c->prim_mol[la] || !c->maxD_mol) return VLXB_EINVAL;",
+          "    vlxb::ExchangeArgs A{};",
+          "    A.mat_K = c->mat; A.pair_i = c->pair_i; A.pair_k = c->pair_k; A.n_ik = c->n_ik;",
+          "    for (int l = 0; l < 3; l++) {",
+          "        A.info[l] = c->prim_info[l]; A.aoinds[l] = c->prim_aoinds[l]; A.count[l] = c->prim_count[l];",
+          "        A.aoinds_col[l] = c->prim_aocols[l];",
+          "    }",
+          "    A.maxD = 0.0; A.D = c->D; A.naos = c->naos; A.D_stride = c->D_stride; A.key_naos = c->naos;",
+          "    A.Q_ab = c->Q_ab; A.Q_cd = c->Q_cd; A.Dinds_ab = c->Dinds_ab; A.Dinds_cd = c->Dinds_cd;",
+          "    A.displs_ab = c->displs_ab; A.displs_cd = c->displs_cd; A.counts_ab = c->counts_ab;",
+          "    A.counts_cd = c->counts_cd; A.pdata_ab = c->pdata_ab; A.pdata_cd = c->pdata_cd;",
+          "    A.omega = c->omega; A.thr = c->thr;",
+          "    A.prim_mol_a = c->prim_mol[la]; A.maxD_mol = c->maxD_mol;",
+          "    switch (la * 27 + lb * 9 + lc * 3 + ld) {"]
+    for cls in k_classes():
+        la, lb, lc, ld = (LV[x] for x in cls)
+        L.append(f"        case {la * 27 + lb * 9 + lc * 3 + ld}: return vlxb::exchange_{cls}(A, (cudaStream_t)stream);")
+    L += ["        default: return VLXB_EINVAL;", "    }", "}", ""]
     L += ["}  // extern \"C\"", ""]
     return "\n".join(L)
 

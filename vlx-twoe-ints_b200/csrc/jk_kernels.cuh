@@ -46,6 +46,7 @@ struct JBraRecs {
     const int32_t* entry;      // [NAB][sp_stride] bra list position or -1
     int64_t sp_stride;
     const double* pdata;       // caller's ab_pair_data (S_ij_00 per bra list position)
+    const int32_t* mol;        // [n_rec] molecule of the record (batched calls), or null
 };
 
 struct JKetPairs {
@@ -58,6 +59,7 @@ struct JKetPairs {
     const double* Dc;    // [NCD][stride] D_kl per component
     int64_t stride;
     const int* n;
+    const int* seg;      // [molecules + 1] ket range of each molecule (batched calls), or null
 };
 
 struct BoysTabs {
@@ -116,17 +118,20 @@ __device__ __forceinline__ void j_quartet(const PairGeo& b, double qb, const JKe
 // Prefix lengths of the descending ket bound list for one bra: ncut (slack
 // included: candidates), nexact (screened-in quartets, for the counters),
 // n64 (bound >= fp32_cut: evaluated in FP64; all of ncut when fp32_cut <= 0).
-__device__ __forceinline__ void ket_prefixes(const JKetPairs& ket, int nket, double qb, double thr,
+// Kets k0 <= t < k1 (one molecule's, sorted by descending bound): ncut / nexact
+// / n64 = end (absolute index) of the kets inside the screening slack band /
+// passing the exact screen / at or above the FP32 cutoff.
+__device__ __forceinline__ void ket_prefixes(const JKetPairs& ket, int k0, int k1, double qb, double thr,
                                              double fp32_cut, int& ncut, int& nexact, int& n64)
 {
-    int lo = 0, hi = nket;
+    int lo = k0, hi = k1;
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
         if (qb * __ldg(ket.tmax + mid) * (1.0 + SCREEN_SLACK) > thr) lo = mid + 1;
         else hi = mid;
     }
     ncut = lo;
-    int lo2 = 0, hi2 = lo;
+    int lo2 = k0, hi2 = lo;
     while (lo2 < hi2) {
         const int mid = (lo2 + hi2) >> 1;
         if (qb * __ldg(ket.tmax + mid) > thr) lo2 = mid + 1;
@@ -136,7 +141,7 @@ __device__ __forceinline__ void ket_prefixes(const JKetPairs& ket, int nket, dou
     if (fp32_cut <= 0.0) {
         n64 = ncut;
     } else {
-        int lo3 = 0, hi3 = ncut;
+        int lo3 = k0, hi3 = ncut;
         while (lo3 < hi3) {
             const int mid = (lo3 + hi3) >> 1;
             if (qb * __ldg(ket.tmax + mid) >= fp32_cut) lo3 = mid + 1;
@@ -168,12 +173,18 @@ coulomb_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double t
         const int sp = __ldg(bra.rec_sp + r);
         const PairGeo b = load_geo(bra.geo, bra.sp_stride, sp);
         const double qb = __ldg(bra.rec_q + r);
+        int k0 = 0, k1 = nket;
+        if (bra.mol) {
+            const int m = __ldg(bra.mol + r);
+            k0 = __ldg(ket.seg + m);
+            k1 = __ldg(ket.seg + m + 1);
+        }
         if (threadIdx.x == 0) {
             int ncut, nexact, n64;
-            ket_prefixes(ket, nket, qb, thr, fp32_cut, ncut, nexact, n64);
+            ket_prefixes(ket, k0, k1, qb, thr, fp32_cut, ncut, nexact, n64);
             s_ncut = ncut;
             s_n64 = n64;
-            if (qcount && PM == 0) atomicAdd(qcount, (unsigned long long)nexact);
+            if (qcount && PM == 0) atomicAdd(qcount, (unsigned long long)(nexact - k0));
         }
         __syncthreads();
         const int ncut = s_ncut, n64 = s_n64;
@@ -186,7 +197,7 @@ coulomb_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double t
 #pragma unroll
         for (int e = 0; e < NE; e++) X[e] = 0.0;
         if (PM == 0) {
-            for (int kt = threadIdx.x; kt < n64; kt += J_THREADS)
+            for (int kt = k0 + threadIdx.x; kt < n64; kt += J_THREADS)
                 j_quartet<LA, LB, LC, LD, double>(b, qb, ket, kt, thr, tabs, X);
         } else {
             for (int kt = n64 + threadIdx.x; kt < ncut; kt += J_THREADS)
@@ -229,6 +240,7 @@ struct KOutBlocks {
     const int32_t* idx;  // [NAC][stride] ik list position or -1
     int64_t stride;
     const int* n;
+    const double* maxD;  // [stride] max |D| bound per block (batched calls), or null: the call's scalar
 };
 
 struct KPartnerRecs {
@@ -403,6 +415,7 @@ exchange_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity dm, d
 
     for (int o = blockIdx.x; o < nout; o += gridDim.x) {
         const int ish = __ldg(out.ish + o), ksh = __ldg(out.ksh + o);
+        const double mD = out.maxD ? __ldg(out.maxD + o) : maxD;
         const int a0 = __ldg(ab.seg + ish), a1 = __ldg(ab.seg + ish + 1);
         const int c0 = __ldg(cd.seg + ksh), c1 = __ldg(cd.seg + ksh + 1);
         double Kacc[NAC];
@@ -411,7 +424,7 @@ exchange_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity dm, d
 
         for (int jb = a0; jb < a1; jb += K_JCHUNK) {
             const int nj = min(K_JCHUNK, a1 - jb);
-            k_chunk_scan(ab, cd, jb, nj, c0, c1, maxD, thr, fp32_cut, ch);
+            k_chunk_scan(ab, cd, jb, nj, c0, c1, mD, thr, fp32_cut, ch);
             const int t64 = s_c64[nj], t32 = s_c32[nj];
             if (qcount && PM == 0 && threadIdx.x == 0) atomicAdd(qcount, (unsigned long long)(t64 + t32));
             if (PM == 0) {

@@ -502,7 +502,8 @@ int contract_groups(Arena& ar, int npa, PairGroups& g, const uint32_t* part_aoin
 
 template <int LC, int LD>
 int jket_prepare(Arena& ar, const PairGroups& g, const uint32_t* first, const uint32_t* second,
-                 const double* D, const double* Q, const double* pdata, JKetData& out)
+                 const double* D, const double* Q, const double* pdata, JKetData& out,
+                 const int32_t* prim_mol_c, int n_mol)
 {
     constexpr int NCD = ncart(LC) * ncart(LD), NF = nrange(LC, LD);
     cudaStream_t st = ar.stream();
@@ -545,6 +546,34 @@ int jket_prepare(Arena& ar, const PairGroups& g, const uint32_t* first, const ui
         VLXB_CHECK_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp, bytes, keys, keys_sorted, perm_in, perm, (int)S,
                                                                   0, 64, st));
     }
+    if (prim_mol_c) {
+        // stable second sort by molecule: per molecule, descending bound
+        int* molkey = ar.alloc<int>(S);
+        int* molkey_sorted = ar.alloc<int>(S);
+        int* perm2 = ar.alloc<int>(S);
+        int* perm_c = ar.alloc<int>(S);
+        double* keys_c = ar.alloc<double>(S);
+        out.seg = ar.alloc<int>(n_mol + 1);
+        if (ar.failed()) return VLXB_ENOMEM;
+        int bits = 1;
+        while ((1 << bits) <= n_mol) bits++;
+        size_t b2 = 0;
+        VLXB_CHECK_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b2, molkey, molkey_sorted, perm_in, perm2, (int)S, 0,
+                                                        bits, st));
+        void* tmp2 = ar.alloc<char>((int64_t)b2);
+        if (!tmp2) return VLXB_ENOMEM;
+        if (!ar.measuring()) {
+            k_jket_molkey<<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, S, perm, g.sp_i, prim_mol_c, n_mol, molkey);
+            VLXB_CHECK_CUDA(cub::DeviceRadixSort::SortPairs(tmp2, b2, molkey, molkey_sorted, perm_in, perm2, (int)S,
+                                                            0, bits, st));
+            k_compose_perm<<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, perm, perm2, keys_sorted, perm_c, keys_c);
+            k_mol_segments<<<prep_blocks(n_mol + 1), PREP_THREADS, 0, st>>>(g.n_sp, molkey_sorted, n_mol, out.seg);
+            note_launches(3);
+        }
+        VLXB_CHECK_CUDA(cudaGetLastError());
+        perm = perm_c;
+        keys_sorted = keys_c;
+    }
     if (!ar.measuring()) {
         k_jket_gather<LC, LD><<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, perm, S, g.geo, keys_sorted, tmin_u,
                                                                        Dpp_u, Dm_u, Qc_u, Dc_u, out.geo, out.tmax,
@@ -556,17 +585,17 @@ int jket_prepare(Arena& ar, const PairGroups& g, const uint32_t* first, const ui
 }
 
 template int jket_prepare<0, 0>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
-                                const double*, const double*, JKetData&);
+                                const double*, const double*, JKetData&, const int32_t*, int);
 template int jket_prepare<0, 1>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
-                                const double*, const double*, JKetData&);
+                                const double*, const double*, JKetData&, const int32_t*, int);
 template int jket_prepare<0, 2>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
-                                const double*, const double*, JKetData&);
+                                const double*, const double*, JKetData&, const int32_t*, int);
 template int jket_prepare<1, 1>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
-                                const double*, const double*, JKetData&);
+                                const double*, const double*, JKetData&, const int32_t*, int);
 template int jket_prepare<1, 2>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
-                                const double*, const double*, JKetData&);
+                                const double*, const double*, JKetData&, const int32_t*, int);
 template int jket_prepare<2, 2>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
-                                const double*, const double*, JKetData&);
+                                const double*, const double*, JKetData&, const int32_t*, int);
 
 template <int NAC>
 static void launch_kout(const uint32_t* pi, const uint32_t* pk, int64_t n, int na, int nc, int npc, const int* spidx,
@@ -577,6 +606,33 @@ static void launch_kout(const uint32_t* pi, const uint32_t* pk, int64_t n, int n
                                                                   out.ksh, out.stride);
     }
     note_launches();
+}
+
+int bra_record_mol(Arena& ar, const PairGroups& g, const int32_t* prim_mol_a, int32_t** mol)
+{
+    *mol = ar.alloc<int32_t>(g.rec_stride);
+    if (!*mol) return VLXB_ENOMEM;
+    if (!ar.measuring()) {
+        k_rec_mol<<<prep_blocks(g.rec_stride), PREP_THREADS, 0, ar.stream()>>>(g.n_rec, g.rec_sp, g.sp_i, prim_mol_a,
+                                                                                *mol);
+        note_launches();
+    }
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    return VLXB_OK;
+}
+
+int kout_block_maxd(Arena& ar, const KOutData& ko, const int32_t* prim_mol_a, const double* maxD_mol,
+                    double** out)
+{
+    *out = ar.alloc<double>(ko.stride);
+    if (!*out) return VLXB_ENOMEM;
+    if (!ar.measuring()) {
+        k_kout_maxd<<<prep_blocks(ko.stride), PREP_THREADS, 0, ar.stream()>>>(ko.n, ko.ish, prim_mol_a, maxD_mol,
+                                                                               *out);
+        note_launches();
+    }
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    return VLXB_OK;
 }
 
 int kout_prepare(Arena& ar, int na, int nc, int npa, int npc, const uint32_t* pi, const uint32_t* pk, int64_t n,

@@ -410,4 +410,65 @@ __global__ void k_grp_order(const int* __restrict__ n_grp, const int* __restrict
     }
 }
 
+// Per-output-block max |D| of batched exchange calls: the block's first
+// primitive shell belongs to one molecule, whose own bound screens the block.
+__global__ void k_kout_maxd(const int* __restrict__ n_blk, const int32_t* __restrict__ ish,
+                            const int32_t* __restrict__ prim_mol, const double* __restrict__ maxD_mol,
+                            double* __restrict__ out)
+{
+    const int n = *n_blk;
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n; o += gridDim.x * blockDim.x)
+        out[o] = maxD_mol[prim_mol[ish[o]]];
+}
+
+// ------------------------------------------------------------ batched Coulomb calls
+// Molecule key of every key-sorted ket (n_mol past the live kets, so they
+// stay last in the stable molecule sort).
+__global__ void k_jket_molkey(const int* __restrict__ n_sp, int64_t S, const int* __restrict__ perm,
+                              const int32_t* __restrict__ sp_i, const int32_t* __restrict__ prim_mol, int n_mol,
+                              int* __restrict__ molkey)
+{
+    const int n = *n_sp;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < S; t += (int64_t)gridDim.x * blockDim.x)
+        molkey[t] = t < n ? prim_mol[sp_i[perm[t]]] : n_mol;
+}
+
+// perm_out[t] = perm[perm2[t]], keys_out[t] = keys[perm2[t]]
+__global__ void k_compose_perm(const int* __restrict__ n_sp, const int* __restrict__ perm,
+                               const int* __restrict__ perm2, const double* __restrict__ keys,
+                               int* __restrict__ perm_out, double* __restrict__ keys_out)
+{
+    const int n = *n_sp;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        perm_out[t] = perm[perm2[t]];
+        keys_out[t] = keys[perm2[t]];
+    }
+}
+
+// seg[m] = first sorted ket of molecule m (molkey ascending over the n_sp live kets)
+__global__ void k_mol_segments(const int* __restrict__ n_sp, const int* __restrict__ molkey, int n_mol,
+                               int* __restrict__ seg)
+{
+    const int n = *n_sp;
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m <= n_mol; m += gridDim.x * blockDim.x) {
+        int lo = 0, hi = n;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (molkey[mid] < m) lo = mid + 1;
+            else hi = mid;
+        }
+        seg[m] = lo;
+    }
+}
+
+// molecule of every bra record
+__global__ void k_rec_mol(const int* __restrict__ n_rec, const int32_t* __restrict__ rec_sp,
+                          const int32_t* __restrict__ sp_i, const int32_t* __restrict__ prim_mol,
+                          int32_t* __restrict__ mol)
+{
+    const int n = *n_rec;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+        mol[r] = prim_mol[sp_i[rec_sp[r]]];
+}
+
 }  // namespace vlxb

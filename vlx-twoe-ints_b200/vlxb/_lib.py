@@ -81,6 +81,18 @@ class Lib:
                                      ctypes.c_int64, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]
         c.vlxb_fockEnergy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                       ctypes.c_void_p, ctypes.c_void_p]
+        c.vlxb_shellPairData.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32,
+                                         ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        c.vlxb_gatherPairDensity.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p,
+                                             ctypes.c_int, ctypes.c_uint32, ctypes.c_int64, ctypes.c_void_p,
+                                             ctypes.c_void_p]
+        c.vlxb_blockMaxAbs.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int64,
+                                       ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
+        for fn in (c.vlxb_coulombBatch, c.vlxb_exchangeBatch):
+            fn.argtypes = [ctypes.c_int] * 4 + [ctypes.c_void_p, ctypes.c_void_p]
+            fn.restype = ctypes.c_int
 
     def check(self, rc: int, what: str):
         if rc != 0:
@@ -135,6 +147,20 @@ class Lib:
     def fock_energy(self, D: int, J: int, K: int, naos: int, out3: int, stream: int = 0):
         """vlxb_fockEnergy on raw device pointers (J or K may be 0 = NULL)."""
         self.check(self.cdll.vlxb_fockEnergy(D, J or None, K or None, int(naos), out3, stream), "vlxb_fockEnergy")
+
+    def shell_pair_data(self, la, lb, info_a, cnt_a, info_b, cnt_b, P, Q, n, S_out, q_out, stream: int = 0):
+        self.check(self.cdll.vlxb_shellPairData(int(la), int(lb), info_a, int(cnt_a), info_b, int(cnt_b), P, Q,
+                                                int(n), S_out, q_out, stream), "vlxb_shellPairData")
+
+    def gather_pair_density(self, D, naos, first, second, ao_a, nca, cnt_a, ao_b, ncb, cnt_b, n, out,
+                            stream: int = 0):
+        self.check(self.cdll.vlxb_gatherPairDensity(D, int(naos), first, second, ao_a, int(nca), int(cnt_a), ao_b,
+                                                    int(ncb), int(cnt_b), int(n), out, stream),
+                   "vlxb_gatherPairDensity")
+
+    def block_max_abs(self, D, naos, rows, nrows, cols, ncols, out, stream: int = 0):
+        self.check(self.cdll.vlxb_blockMaxAbs(D, int(naos), rows, int(nrows), cols, int(ncols), out, stream),
+                   "vlxb_blockMaxAbs")
 
     def reset_counters(self, stream: int = 0):
         self.check(self.cdll.vlxb_quartetCounters(None, 1, stream), "vlxb_quartetCounters")

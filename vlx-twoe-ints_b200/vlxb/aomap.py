@@ -80,16 +80,46 @@ def contract_host(naos: int, values: np.ndarray, rowptr, row_ao, src) -> np.ndar
     return M
 
 
+def build_map_torch(naos: int, parts):
+    """build_map on tensors (same layout and entry order): parts are
+    (offset, a, b, diag_entry) with int64 / bool tensors.  Returns tensors
+    (rowptr int64, row_ao int32, src int32 holding the uint32 bits)."""
+    dev = parts[0][1].device if parts else torch.device("cpu")
+    rows, srcs = [], []
+    for off, a, b, de in parts:
+        lo, hi = torch.minimum(a, b), torch.maximum(a, b)
+        pos = off + torch.arange(a.numel(), dtype=torch.int64, device=dev)
+        if pos.numel() and int(pos[-1]) >= (1 << 31):
+            raise ValueError("more than 2^31 pair values")
+        rows.append(lo * naos + hi)
+        srcs.append(pos | (((a == b) & ~de).to(torch.int64) << 31))
+    if not rows:
+        return (torch.zeros(1, dtype=torch.int64, device=dev), torch.zeros(0, dtype=torch.int32, device=dev),
+                torch.zeros(0, dtype=torch.int32, device=dev))
+    row = torch.cat(rows)
+    src = torch.cat(srcs)
+    order = torch.sort(row, stable=True).indices  # positions ascend within a row: the concatenation order
+    row, src = row[order], src[order]
+    uniq, cnt = torch.unique_consecutive(row, return_counts=True)
+    rowptr = torch.zeros(uniq.numel() + 1, dtype=torch.int64, device=dev)
+    rowptr[1:] = torch.cumsum(cnt, 0)
+    src32 = torch.where(src >= (1 << 31), src - (1 << 32), src).to(torch.int32)  # uint32 bits in int32 storage
+    return rowptr, uniq.to(torch.int32), src32
+
+
 class _DeviceMap:
     def __init__(self, keys, sizes, rowptr, row_ao, src, device):
         self.keys = list(keys)
         self.sizes = list(sizes)
         self.offsets = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int64)
         self.total = int(self.offsets[-1])
-        self.rowptr = torch.from_numpy(rowptr).to(device)
-        self.row_ao = torch.from_numpy(row_ao).to(device)
-        self.src = torch.from_numpy(src.view(np.int32)).to(device)
-        self.n_rows = len(row_ao)
+        if isinstance(rowptr, torch.Tensor):
+            self.rowptr, self.row_ao, self.src = rowptr.to(device), row_ao.to(device), src.to(device)
+        else:
+            self.rowptr = torch.from_numpy(rowptr).to(device)
+            self.row_ao = torch.from_numpy(row_ao).to(device)
+            self.src = torch.from_numpy(src.view(np.int32)).to(device)
+        self.n_rows = int(self.row_ao.numel())
 
     def alloc(self, device):
         """Zeroed flat value buffer and per-list views into it."""
@@ -117,6 +147,36 @@ class AOMap:
         kmap = build_map(self.naos, [(koff[i], *_targets_K(rl, k)) for i, k in enumerate(kkeys)])
         self.J = _DeviceMap(jkeys, jsz, *jmap, self.device)
         self.K = _DeviceMap(kkeys, ksz, *kmap, self.device)
+
+    @classmethod
+    def from_device(cls, dl) -> "AOMap":
+        """The map of device-resident lists (fock.DeviceLists), built where they live."""
+        self = cls.__new__(cls)
+        self.device = dl.device
+        self.naos = dl.naos
+
+        def ao(l, idx):
+            n = NCART[l]
+            idx = idx.long()
+            return dl.aoinds[l][idx % n, idx // n].long()
+
+        jkeys, kkeys = sorted(dl.j), sorted(dl.kpair)
+        jsz = [dl.j[k]["first"].numel() for k in jkeys]
+        ksz = [dl.kpair[k]["i"].numel() for k in kkeys]
+        joff = np.concatenate([[0], np.cumsum(jsz)]).astype(np.int64)
+        koff = np.concatenate([[0], np.cumsum(ksz)]).astype(np.int64)
+        jp, kp = [], []
+        for t, k in enumerate(jkeys):
+            la, lb = LV[k[0]], LV[k[1]]
+            f, s2 = dl.j[k]["first"], dl.j[k]["second"]
+            jp.append((int(joff[t]), ao(la, f), ao(lb, s2), (f == s2) & (la == lb)))
+        for t, k in enumerate(kkeys):
+            la, lc = LV[k[0]], LV[k[1]]
+            i, kk = dl.kpair[k]["i"], dl.kpair[k]["k"]
+            kp.append((int(koff[t]), ao(la, i), ao(lc, kk), (i == kk) & (la == lc)))
+        self.J = _DeviceMap(jkeys, jsz, *build_map_torch(self.naos, jp), self.device)
+        self.K = _DeviceMap(kkeys, ksz, *build_map_torch(self.naos, kp), self.device)
+        return self
 
     def alloc_outputs(self):
         """(flatJ, matJ views, flatK, matK views): pass the views to build_jk."""
@@ -149,4 +209,4 @@ def energy(D: torch.Tensor, J: torch.Tensor | None, K: torch.Tensor | None, out:
     return out
 
 
-__all__ = ["AOMap", "build_map", "contract_host", "energy"]
+__all__ = ["AOMap", "build_map", "build_map_torch", "contract_host", "energy"]
