@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--batch-atoms", type=int, nargs=2, default=(3, 8), help="batched leg: atom count range")
     ap.add_argument("--serve-reqs", type=int, default=16, help="served leg: requests (0 skips the leg)")
     ap.add_argument("--serve-atoms", type=int, nargs=2, default=(5, 12), help="served leg: atom count range")
-    ap.add_argument("--serve-iters", type=int, default=4, help="served leg: densities per request")
+    ap.add_argument("--serve-iters", type=int, default=10, help="served leg: densities per request")
     ap.add_argument("--serve-rate", type=float, default=50.0, help="served leg: Poisson arrival rate (req/s)")
     return ap.parse_args()
 

@@ -17,6 +17,9 @@ J and K stay on the device: the prim-pair outputs are contracted to AO
 matrices by vlxb_pairsToAO, incremental updates are added there, and only
 the energy terms (vlxb_fockEnergy, three doubles) are read back per build;
 the AO J and K of a request are copied to the host once, when it finishes.
+With device_lists (the default) the lists themselves are built on the GPU at
+admission (vlxb.devlists) and refreshed there for every new density, so the
+host only uploads each density and reads back three doubles per build.
 
 Results are deterministic: the kernels have no atomics on J/K, so a request
 gives the same J/K alone and in any mix (tested).
@@ -31,7 +34,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from . import aomap, fock, lists
+from . import aomap, devlists, fock, lists
 from ._lib import lib
 
 
@@ -64,15 +67,17 @@ def perturbed_densities(D0: np.ndarray, n: int, rng: np.random.Generator, hi: fl
 class _Active:
     def __init__(self, req, rl, dl, stream, incremental):
         self.req = req
-        self.rl = rl
+        self.rl = rl          # host lists, or None when the lists live on the device only
         self.dl = dl
         self.stream = stream
         self.incremental = incremental
         self.it = 0
         self.prevD = None
-        n = rl.naos
+        n = dl.naos
         with torch.cuda.stream(stream):
-            self.am = aomap.AOMap(rl, dl.device)
+            self.am = aomap.AOMap(rl, dl.device) if rl is not None else aomap.AOMap.from_device(dl)
+            self.prevDdev = torch.zeros((n, n), dtype=torch.float64, device=dl.device)
+            self.useDdev = torch.empty_like(self.prevDdev)
             self.flatJ, self.matJ, self.flatK, self.matK = self.am.alloc_outputs()
             self.J = torch.zeros((n, n), dtype=torch.float64, device=dl.device)   # running AO J
             self.K = torch.zeros((n, n), dtype=torch.float64, device=dl.device)
@@ -87,7 +92,7 @@ class _Active:
 
 class Server:
     def __init__(self, budget_bytes: float = 120e9, max_active: int = 16, device="cuda", fp32_cut: float = 0.0,
-                 incremental: bool = False, prep_workers: int = 2):
+                 incremental: bool = False, prep_workers: int = 2, device_lists: bool = True):
         self.budget = float(budget_bytes)
         self.max_active = max_active
         self.device = torch.device(device)
@@ -95,10 +100,13 @@ class Server:
         self.L.init(self.device.index or 0)
         self.fp32_cut = fp32_cut
         self.incremental = incremental
+        self.device_lists = device_lists
         self.pool = cf.ThreadPoolExecutor(max_workers=prep_workers)
         self.schwarz = fock.gpu_schwarz_fn(self.device)
 
     def _prepare(self, req):
+        if self.device_lists:
+            return None  # built on the GPU at admission
         return lists.build_lists(req.mol, req.densities[0], req.threshold, self.schwarz)
 
     @staticmethod
@@ -125,9 +133,17 @@ class Server:
         its read-back."""
         D = a.req.densities[a.it]
         inc = a.incremental and a.prevD is not None
-        use = D - a.prevD if inc else D
         with torch.cuda.stream(a.stream):
-            self._set_density(a.rl, a.dl, use)
+            a.Ddev.copy_(torch.from_numpy(np.ascontiguousarray(D)))
+            if a.rl is None:
+                if inc:
+                    torch.sub(a.Ddev, a.prevDdev, out=a.useDdev)
+                    devlists.set_density(a.dl, a.useDdev, stream=a.stream)
+                else:
+                    devlists.set_density(a.dl, a.Ddev, stream=a.stream)
+                a.prevDdev.copy_(a.Ddev)
+            else:
+                self._set_density(a.rl, a.dl, D - a.prevD if inc else D)
             a.flatJ.zero_()
             a.flatK.zero_()
             fock.build_jk(a.dl, stream=a.stream, matJ=a.matJ, matK=a.matK)
@@ -139,7 +155,6 @@ class Server:
             else:
                 a.am.to_ao("J", a.flatJ, out=a.J, stream=a.stream)
                 a.am.to_ao("K", a.flatK, out=a.K, stream=a.stream)
-            a.Ddev.copy_(torch.from_numpy(np.ascontiguousarray(D)))
             aomap.energy(a.Ddev, a.J, a.K, out=a.e_dev, stream=a.stream)
             a.e_host.copy_(a.e_dev, non_blocking=True)
             ev = torch.cuda.Event()
@@ -178,11 +193,20 @@ class Server:
                     if not fut.done() or len(active) >= self.max_active:
                         continue
                     rl = fut.result()
-                    est = 1.5 * sum(x.nbytes for x in fock.host_arrays(rl).values())
+                    if rl is not None:
+                        est = 1.5 * sum(x.nbytes for x in fock.host_arrays(rl).values())
+                    else:  # bound on the device lists: all primitive pairs of all type pairs
+                        n = r.mol.naos
+                        est = 8.0 * 64 * n * n
                     if resident + est > self.budget and active:
                         continue
-                    dl = fock.to_device(rl, self.device)
-                    a = _Active(r, rl, dl, torch.cuda.Stream(device=self.device), self.incremental)
+                    st = torch.cuda.Stream(device=self.device)
+                    if rl is not None:
+                        dl = fock.to_device(rl, self.device)
+                    else:
+                        with torch.cuda.stream(st):
+                            dl = devlists.build_device_lists(r.mol, r.densities[0], r.threshold, self.device)
+                    a = _Active(r, rl, dl, st, self.incremental)
                     r.admitted = time.perf_counter() - t0
                     resident += a.bytes
                     active.append(a)
