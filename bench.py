@@ -194,16 +194,18 @@ def cpu_reference(rl, budget_s, seed=0):
         n = len(rl.jlists[cls[:2]].first) if kind == "J" else len(rl.kpairs[cls[0] + cls[2]].pair_i)
         nrow = min(n, max(threads, 1))
         rows = np.sort(rng.choice(n, size=nrow, replace=False)).astype(np.uint32)
-        # pilot to size the per-row evaluation cap
+        # grow the per-row evaluation cap until the sample takes a fair share
+        # of the class's time budget (or every passing quartet is evaluated),
+        # so per-call overhead does not bias the measured throughput
         f = ref.coulomb if kind == "J" else ref.exchange
-        t0 = time.perf_counter()
-        _, p_pass, p_eval = f(rl, cls, rows=rows, max_eval=8)
-        dt = max(time.perf_counter() - t0, 1e-6)
-        rate = max(p_eval, 1) / dt
-        cap = int(max(8, min(2**40, rate * per / max(nrow, 1))))
-        t0 = time.perf_counter()
-        _, c_pass, c_eval = f(rl, cls, rows=rows, max_eval=cap)
-        dt = max(time.perf_counter() - t0, 1e-6)
+        cap = 64
+        while True:
+            t0 = time.perf_counter()
+            _, c_pass, c_eval = f(rl, cls, rows=rows, max_eval=cap)
+            dt = max(time.perf_counter() - t0, 1e-6)
+            if dt >= 0.25 * per or c_eval < cap * nrow or cap >= 2**40:
+                break
+            cap = int(min(2**40, cap * max(2.0, min(64.0, 0.5 * per / dt))))
         thr = max(c_eval, 1) / dt  # component quartets per second, whole machine
         est_total += (c_pass / nrow) * n / thr
         cq_eval_total += c_eval

@@ -242,9 +242,10 @@ def _k_variants(cls):
     return out
 
 
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, 2])
 def test_golden_every_coulomb_variant(golden, variant):
-    """Both Coulomb kernels (thread per quartet, warp column) on every class."""
+    """Every Coulomb kernel (thread per quartet, warp column, McMurchie-Davidson)
+    on every class."""
     z = golden
     L = lib()
     saved = {c: L.get_schedule("J", c) for c in tf.j_classes()}
@@ -358,3 +359,39 @@ def test_contracted_exchange_variants_vs_oracle(variant):
     finally:
         for c, v in saved.items():
             L.set_schedule("K", c, v)
+
+
+def test_md_coulomb_vs_oracle_and_counts():
+    """The McMurchie-Davidson Coulomb kernel (variant 2) on every class of a
+    degree-3 s/p/d system: AO J within 1e-10 of the FP64 oracle, quartet
+    counts equal to the thread kernel's, and its FP32 pass within the mixed
+    tolerance of its FP64 result."""
+    L = lib()
+    L.init(0)
+    wl = basis.config_custom(3, 4.0, {0: 2, 1: 1, 2: 1}, 3, 0.2, 2.5, 3, 1e-12, 23)
+    rl = lists.build_lists(wl.mol, wl.D, wl.threshold, fock.gpu_schwarz_fn())
+    dl = fock.to_device(rl)
+    saved = {c: L.get_schedule("J", c) for c in lists.j_classes()}
+    try:
+        res = {}
+        for v in (0, 2):
+            for c in lists.j_classes():
+                L.set_schedule("J", c, v)
+            L.reset_counters()
+            mJ, _ = fock.build_jk(dl, do_k=False)
+            torch.cuda.synchronize()
+            res[v] = (lists.contract_J(rl, {k: t.cpu().numpy() for k, t in mJ.items()}), L.quartet_counters()[0])
+        oJ, _ = helpers.oracle_jk_all(rl)
+        Jo = lists.contract_J(rl, oJ)
+        assert np.abs(res[2][0] - Jo).max() <= 1e-10 * max(1.0, np.abs(Jo).max())
+        assert res[2][1] == res[0][1]
+        L.set_fp32_cut(1e-6)
+        mJ, _ = fock.build_jk(dl, do_k=False)
+        torch.cuda.synchronize()
+        L.set_fp32_cut(0.0)
+        J32 = lists.contract_J(rl, {k: t.cpu().numpy() for k, t in mJ.items()})
+        assert np.abs(J32 - res[2][0]).max() <= 1e-7
+    finally:
+        L.set_fp32_cut(0.0)
+        for c, v in saved.items():
+            L.set_schedule("J", c, v)

@@ -4,6 +4,7 @@
 #include "col_kernels.cuh"
 #include "engine.cuh"
 #include "jk_kernels.cuh"
+#include "md_kernels.cuh"
 
 namespace vlxb {
 
@@ -84,8 +85,9 @@ int run_coulomb_impl(const CoulombArgs& a, cudaStream_t st, Arena& ar, const Boy
     if (rc) return rc;
     const bool batched = a.prim_mol_a && a.prim_mol_c && a.n_mol > 0;
     JKetData kd;
+    const int jvar = schedule_get(0, LA, LB, LC, LD);
     rc = jket_prepare<LC, LD>(ar, gk, a.cd_first, a.cd_second, a.cd_D, a.cd_Q, a.cd_pdata, kd,
-                              batched ? a.prim_mol_c : nullptr, batched ? a.n_mol : 0);
+                              batched ? a.prim_mol_c : nullptr, batched ? a.n_mol : 0, jvar == 2);
     if (rc) return rc;
     int32_t* bmol = nullptr;
     if (batched) {
@@ -95,20 +97,31 @@ int run_coulomb_impl(const CoulombArgs& a, cudaStream_t st, Arena& ar, const Boy
     if (ar.failed()) return VLXB_ENOMEM;
     if (ar.measuring()) return VLXB_OK;
     JBraRecs bra{gb.rec_sp, gb.rec_q, gb.rec_mask, gb.n_rec, gb.geo, gb.entry, gb.sp_stride, a.ab_pdata, bmol};
-    JKetPairs ket{kd.geo, kd.tmax, kd.tmin, kd.Dpp, kd.Dm, kd.Qc, kd.Dc, kd.stride, kd.n, batched ? kd.seg : nullptr};
+    JKetPairs ket{kd.geo, kd.tmax, kd.tmin, kd.Dpp, kd.Dm, kd.Qc, kd.Dc, kd.stride, kd.n, batched ? kd.seg : nullptr,
+                  kd.Dh};
     int grid = launch_grid_limit();
     if ((int64_t)grid > (int64_t)a.n_ab) grid = (int)a.n_ab;
-    const bool col = schedule_get(0, LA, LB, LC, LD) == 1;
-    if (col)
-        coulomb_col_kernel<LA, LB, LC, LD, 0><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut);
-    else
-        coulomb_kernel<LA, LB, LC, LD, 0><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut);
-    note_launches();
-    if (cut > 0.0) {
-        if (col)
-            coulomb_col_kernel<LA, LB, LC, LD, 1><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut);
-        else
-            coulomb_kernel<LA, LB, LC, LD, 1><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut);
+    for (int pm = 0; pm < (cut > 0.0 ? 2 : 1); pm++) {
+        if (jvar == 2) {
+            if (pm == 0)
+                coulomb_md_kernel<LA, LB, LC, LD, 0><<<grid, MD_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc,
+                                                                                  cut);
+            else
+                coulomb_md_kernel<LA, LB, LC, LD, 1><<<grid, MD_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc,
+                                                                                  cut);
+        } else if (jvar == 1) {
+            if (pm == 0)
+                coulomb_col_kernel<LA, LB, LC, LD, 0><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc,
+                                                                                  cut);
+            else
+                coulomb_col_kernel<LA, LB, LC, LD, 1><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc,
+                                                                                  cut);
+        } else {
+            if (pm == 0)
+                coulomb_kernel<LA, LB, LC, LD, 0><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut);
+            else
+                coulomb_kernel<LA, LB, LC, LD, 1><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut);
+        }
         note_launches();
     }
     VLXB_CHECK_CUDA(cudaGetLastError());

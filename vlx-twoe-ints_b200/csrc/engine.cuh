@@ -170,13 +170,14 @@ struct JKetData {
     int64_t stride;
     int* n;
     int* seg = nullptr;  // [n_mol + 1] ket offsets per molecule (batched calls)
+    double* Dh = nullptr;  // [stride][nherm(LC + LD)] Hermite ket density (McMurchie-Davidson kernel)
 };
 // prim_mol_c (batched calls, else null): molecule of every type-c primitive;
 // the kets are then sorted by molecule, and by descending bound inside one.
 template <int LC, int LD>
 int jket_prepare(Arena& ar, const PairGroups& g, const uint32_t* first, const uint32_t* second,
                  const double* D, const double* Q, const double* pdata, JKetData& out,
-                 const int32_t* prim_mol_c = nullptr, int n_mol = 0);
+                 const int32_t* prim_mol_c = nullptr, int n_mol = 0, bool hermite = false);
 // Molecule of every bra record (batched Coulomb calls).
 int bra_record_mol(Arena& ar, const PairGroups& g, const int32_t* prim_mol_a, int32_t** mol);
 

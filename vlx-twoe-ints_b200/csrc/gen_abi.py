@@ -141,7 +141,8 @@ def header():
          "   DFMA peak.  No reference counterpart. */",
          "int vlxb_fp64Probe(double* out, int iters, int blocks, void* stream);", "",
          "/* Kernel variant used for one class (kind 0 = Coulomb: 0 one thread per",
-         "   shell quartet, 1 warp-cooperative column kernel; kind 1 = exchange: 0",
+         "   shell quartet, 1 warp-cooperative column kernel, 2 McMurchie-Davidson",
+         "   kernel (Hermite ket densities, one quartet per warp); kind 1 = exchange: 0",
          "   one thread per quartet, 1 column kernel with bra lanes, 2 column kernel",
          "   with ket lanes, 3 / 4 the column kernels with bra / ket lanes that sum",
          "   the primitive partners of one contracted shell before the HRR).  A",

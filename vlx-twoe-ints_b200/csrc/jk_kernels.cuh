@@ -60,6 +60,7 @@ struct JKetPairs {
     int64_t stride;
     const int* n;
     const int* seg;      // [molecules + 1] ket range of each molecule (batched calls), or null
+    const double* Dh;    // [stride][nherm(LC+LD)] Hermite ket density (McMurchie-Davidson kernel), or null
 };
 
 struct BoysTabs {

@@ -151,7 +151,7 @@ int schedule_set(int kind, int la, int lb, int lc, int ld, int variant)
 {
     if (kind < 0 || kind > 1 || la < 0 || la > 2 || lb < 0 || lb > 2 || lc < 0 || lc > 2 || ld < 0 || ld > 2)
         return VLXB_EINVAL;
-    if (variant < 0 || variant > (kind == 0 ? 1 : 4)) return VLXB_EINVAL;
+    if (variant < 0 || variant > (kind == 0 ? 2 : 4)) return VLXB_EINVAL;
     std::call_once(g_sched_once, sched_init);
     g_sched[kind][la * 27 + lb * 9 + lc * 3 + ld].store(variant);
     return VLXB_OK;
@@ -503,7 +503,7 @@ int contract_groups(Arena& ar, int npa, PairGroups& g, const uint32_t* part_aoin
 template <int LC, int LD>
 int jket_prepare(Arena& ar, const PairGroups& g, const uint32_t* first, const uint32_t* second,
                  const double* D, const double* Q, const double* pdata, JKetData& out,
-                 const int32_t* prim_mol_c, int n_mol)
+                 const int32_t* prim_mol_c, int n_mol, bool hermite)
 {
     constexpr int NCD = ncart(LC) * ncart(LD), NF = nrange(LC, LD);
     cudaStream_t st = ar.stream();
@@ -581,21 +581,30 @@ int jket_prepare(Arena& ar, const PairGroups& g, const uint32_t* first, const ui
     }
     if (!ar.measuring()) note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
+    if (hermite) {
+        out.Dh = ar.alloc<double>(S * nherm(LC + LD));
+        if (!out.Dh) return VLXB_ENOMEM;
+        if (!ar.measuring()) {
+            k_jket_hermite<LC, LD><<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, S, out.geo, out.Dm, out.Dh);
+            note_launches();
+        }
+        VLXB_CHECK_CUDA(cudaGetLastError());
+    }
     return VLXB_OK;
 }
 
 template int jket_prepare<0, 0>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
-                                const double*, const double*, JKetData&, const int32_t*, int);
+                                const double*, const double*, JKetData&, const int32_t*, int, bool);
 template int jket_prepare<0, 1>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
-                                const double*, const double*, JKetData&, const int32_t*, int);
+                                const double*, const double*, JKetData&, const int32_t*, int, bool);
 template int jket_prepare<0, 2>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
-                                const double*, const double*, JKetData&, const int32_t*, int);
+                                const double*, const double*, JKetData&, const int32_t*, int, bool);
 template int jket_prepare<1, 1>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
-                                const double*, const double*, JKetData&, const int32_t*, int);
+                                const double*, const double*, JKetData&, const int32_t*, int, bool);
 template int jket_prepare<1, 2>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
-                                const double*, const double*, JKetData&, const int32_t*, int);
+                                const double*, const double*, JKetData&, const int32_t*, int, bool);
 template int jket_prepare<2, 2>(Arena&, const PairGroups&, const uint32_t*, const uint32_t*, const double*,
-                                const double*, const double*, JKetData&, const int32_t*, int);
+                                const double*, const double*, JKetData&, const int32_t*, int, bool);
 
 template <int NAC>
 static void launch_kout(const uint32_t* pi, const uint32_t* pk, int64_t n, int na, int nc, int npc, const int* spidx,

@@ -15,6 +15,7 @@
 // kernels read it), so a whole ABI call issues no host synchronisation.
 #pragma once
 #include "common.cuh"
+#include "md.cuh"
 
 namespace vlxb {
 
@@ -469,6 +470,23 @@ __global__ void k_rec_mol(const int* __restrict__ n_rec, const int32_t* __restri
     const int n = *n_rec;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
         mol[r] = prim_mol[sp_i[rec_sp[r]]];
+}
+
+// Signed Hermite density of every sorted ket pair (McMurchie-Davidson Coulomb
+// kernel), stored per ket: Dh[kt * nherm(LC + LD) + f].
+template <int LC, int LD>
+__global__ void k_jket_hermite(const int* __restrict__ n_sp, int64_t stride, const double* __restrict__ geo,
+                               const double* __restrict__ Dm, double* __restrict__ Dh)
+{
+    constexpr int NCD = ncart(LC) * ncart(LD), NH = nherm(LC + LD);
+    const int n = *n_sp;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const PairGeo k = load_geo(geo, stride, r);
+        double dm[NCD], dh[NH];
+        for (int c = 0; c < NCD; c++) dm[c] = Dm[c * stride + r];
+        herm_ket_density<LC, LD, double>(k, dm, dh);
+        for (int f = 0; f < NH; f++) Dh[(int64_t)r * NH + f] = dh[f];
+    }
 }
 
 }  // namespace vlxb

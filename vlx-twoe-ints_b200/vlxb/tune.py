@@ -37,7 +37,7 @@ def compiled_variants(kind: str, cls: str):
     from gen_column import ColumnPlan, k_smem_bytes
 
     if kind == "J":
-        return [1] if cls in SPILLING_THREAD_KERNELS["J"] else [0, 1]
+        return [1, 2] if cls in SPILLING_THREAD_KERNELS["J"] else [0, 1, 2]
     l = [{"s": 0, "p": 1, "d": 2}[x] for x in cls]
     out = [] if cls in SPILLING_THREAD_KERNELS["K"] else [0]
     for ori in (0, 1):
