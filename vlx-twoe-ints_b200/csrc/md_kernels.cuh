@@ -45,6 +45,7 @@ coulomb_md_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, doubl
     __shared__ double sEk[NW][3][NEK];  // ket 1-D Hermite coefficients (slack-band kets)
     __shared__ double sDm[NW][NCD];     // screened ket density (slack-band kets)
     __shared__ double sEb[3][NEB];      // bra 1-D Hermite coefficients
+    __shared__ T sBase[NW][L + 1];      // R^{(n)}_{000} of the warp's quartet
     __shared__ int s_ncut, s_n64;
 
     for (int i = threadIdx.x; i < NHL; i += MD_THREADS) {
@@ -172,7 +173,11 @@ coulomb_md_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, doubl
             const T X_ = (T)PQx, Y_ = (T)PQy, Z_ = (T)PQz;
             T* R0 = sR[warp][0];
             T* R1 = sR[warp][1];
-            if (lane == 0) R0[0] = base[L];
+            if (lane == 0) {
+#pragma unroll
+                for (int n = 0; n <= L; n++) sBase[warp][n] = base[n];
+                R0[0] = base[L];
+            }
             __syncwarp();
 #pragma unroll 1
             for (int n = L - 1; n >= 0; n--) {
@@ -185,7 +190,7 @@ coulomb_md_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, doubl
                     const T pq = dir == 0 ? X_ : (dir == 1 ? Y_ : Z_);
                     T val = pq * src[rec & 1023u];
                     if (s2 != 1023u) val = fma((T)((rec >> 20) & 255u), src[s2], val);
-                    dst[i] = i == 0 ? base[n] : val;
+                    dst[i] = i == 0 ? sBase[warp][n] : val;
                 }
                 __syncwarp();
             }
