@@ -141,7 +141,8 @@ def dist_setup():
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         import datetime
 
-        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        if not dist.is_initialized():
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
     return ws, rank, local
 
 
