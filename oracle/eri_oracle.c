@@ -19,6 +19,9 @@
  *   - Range separation: d2 = w^2/(rho + w^2), Lambda *= sqrt(d2),
  *     T *= d2, F_m *= d2^m: gen_exchange.py:278-298.
  *   - J digestion with the k<->l doubling weights: gen_coulomb.py:205-297.
+ *   - Bra-centre derivatives of J (Coulomb nuclear gradient) by the
+ *     Obara-Saika derivative relation, the generator's gradient='a' / 'b'
+ *     terms (eri.py:85-129), on the same integrals and digestion.
  *   - K digestion over partner lists with the max-D screen and the AO-density
  *     gather: gen_exchange.py:139-342.
  * Screening follows the set semantics that the reference's per-thread
@@ -42,7 +45,6 @@
 
 #define OR_MAXL 4          /* max angular momentum of one e or f index     */
 #define OR_MAXM 16         /* max Boys order                               */
-#define OR_NCI 125         /* (OR_MAXL+1)^3 Cartesian triplet slots        */
 
 static const long double OR_PI_L = 3.141592653589793238462643383279502884L;
 
@@ -83,18 +85,19 @@ typedef struct {
     double PA[3], WP[3], QC[3], WQ[3], AB[3], CD[3];
     double inv2z, inv2e, inv2ze, rho_z, rho_e;
     double base[OR_MAXM + 1];
-    double* memo;      /* OR_NCI * OR_NCI * (OR_MAXM+1) values */
+    double* memo;      /* nci * nci * (OR_MAXM+1) values */
     uint32_t* stamp;   /* same shape */
     uint32_t cur;
+    int nb, nci;       /* Cartesian triplet slots: components 0..nb-1, nci = nb^3 */
 } OrCtx;
 
-static inline int ci(const int v[3]) { return v[0] * 25 + v[1] * 5 + v[2]; }
+static inline int ci(const OrCtx* c, const int v[3]) { return (v[0] * c->nb + v[1]) * c->nb + v[2]; }
 
 static double vrr(OrCtx* c, const int e[3], const int f[3], int m)
 {
     if (e[0] < 0 || e[1] < 0 || e[2] < 0 || f[0] < 0 || f[1] < 0 || f[2] < 0)
         return 0.0;
-    size_t key = ((size_t)ci(e) * OR_NCI + (size_t)ci(f)) * (OR_MAXM + 1) + (size_t)m;
+    size_t key = ((size_t)ci(c, e) * c->nci + (size_t)ci(c, f)) * (OR_MAXM + 1) + (size_t)m;
     if (c->stamp[key] == c->cur) return c->memo[key];
     double v;
     if (f[0] + f[1] + f[2] > 0) {
@@ -188,18 +191,24 @@ static void setup_quartet(OrCtx* c, int L, double ai, const double* Ai, double a
     double dm = 1.0;
     for (int m = 0; m <= L; m++) { c->base[m] = lam * F[m] * dm; dm *= d2; }
     c->cur++;
-    if (c->cur == 0) { memset(c->stamp, 0, sizeof(uint32_t) * (size_t)OR_NCI * OR_NCI * (OR_MAXM + 1)); c->cur = 1; }
+    if (c->cur == 0) { memset(c->stamp, 0, sizeof(uint32_t) * (size_t)c->nci * c->nci * (OR_MAXM + 1)); c->cur = 1; }
 }
 
-static OrCtx* ctx_new(void)
+/* nb = 1 + the largest Cartesian exponent an e or f index reaches: OR_MAXL + 1
+   for (ab|cd) over s, p, d; one more for the derivative integrals. */
+static OrCtx* ctx_new_nb(int nb)
 {
     OrCtx* c = (OrCtx*)calloc(1, sizeof(OrCtx));
-    size_t n = (size_t)OR_NCI * OR_NCI * (OR_MAXM + 1);
+    c->nb = nb;
+    c->nci = nb * nb * nb;
+    size_t n = (size_t)c->nci * c->nci * (OR_MAXM + 1);
     c->memo = (double*)malloc(sizeof(double) * n);
     c->stamp = (uint32_t*)calloc(n, sizeof(uint32_t));
     c->cur = 0;
     return c;
 }
+
+static OrCtx* ctx_new(void) { return ctx_new_nb(OR_MAXL + 1); }
 
 static void ctx_free(OrCtx* c) { free(c->memo); free(c->stamp); free(c); }
 
@@ -295,6 +304,69 @@ void oracle_coulomb_fock(int la, int lb, int lc, int ld, double* mat_J,
                 J += eri * cd_mat_D[kl] * w8;
             }
             mat_J[ij] += J;
+        }
+        ctx_free(c);
+    }
+}
+
+/* Bra-centre derivatives of J for one (ab|cd) class: the derivative of
+   oracle_coulomb_fock's mat_J[ij] with respect to the centres A (first) and
+   B (second) of bra entry ij, kets and cd_mat_D fixed, by the Obara-Saika
+   derivative relation of a Cartesian Gaussian (Obara & Saika 1986, Eq. 5; the
+   generator's gradient='a' / 'b' terms, eri.py:85-129):
+     d/dA_x (a b|c d) = 2 alpha (a+1x b|c d) - a_x (a-1x b|c d),
+     d/dB_x (a b|c d) = 2 beta  (a b+1x|c d) - b_x (a b-1x|c d).
+   grad_J[k * gstride + ij] +=, k = 0..2 for A_x..A_z, 3..5 for B_x..B_z.
+   Same screening and ket weights as oracle_coulomb_fock. */
+void oracle_coulomb_grad(int la, int lb, int lc, int ld, double* grad_J, uint64_t gstride,
+                         const double* const* prim_info, const uint32_t* prim_count,
+                         const double* cd_mat_D, const double* ab_mat_Q, const double* cd_mat_Q,
+                         const uint32_t* ab_first, const uint32_t* ab_second,
+                         const double* ab_pair_data, uint32_t n_ab,
+                         const uint32_t* cd_first, const uint32_t* cd_second,
+                         const double* cd_pair_data, uint32_t n_cd,
+                         double thr, const uint32_t* rows, uint32_t nrows)
+{
+    uint32_t nwork = rows ? nrows : n_ab;
+    int L = la + lb + lc + ld + 1;
+    #pragma omp parallel
+    {
+        OrCtx* c = ctx_new_nb(OR_MAXL + 2);
+        #pragma omp for schedule(dynamic, 4)
+        for (int64_t w = 0; w < (int64_t)nwork; w++) {
+            uint32_t ij = rows ? rows[w] : (uint32_t)w;
+            double ai, aj, ri[3], rj[3];
+            int ca, cb;
+            prim_of(prim_info[la], prim_count[la], la, ab_first[ij], &ai, ri, &ca);
+            prim_of(prim_info[lb], prim_count[lb], lb, ab_second[ij], &aj, rj, &cb);
+            const int* a = cart_comp(la, ca);
+            const int* b = cart_comp(lb, cb);
+            double g[6] = {0, 0, 0, 0, 0, 0};
+            for (uint32_t kl = 0; kl < n_cd; kl++) {
+                if (fabs(ab_mat_Q[ij] * cd_mat_Q[kl] * cd_mat_D[kl]) <= thr) continue;
+                double ak, al, rk[3], rl[3];
+                int cc, cd;
+                uint32_t k = cd_first[kl], l = cd_second[kl];
+                prim_of(prim_info[lc], prim_count[lc], lc, k, &ak, rk, &cc);
+                prim_of(prim_info[ld], prim_count[ld], ld, l, &al, rl, &cd);
+                setup_quartet(c, L, ai, ri, aj, rj, ak, rk, al, rl, 0.0);
+                const int* kc = cart_comp(lc, cc);
+                const int* kd = cart_comp(ld, cd);
+                double w8 = (lc != ld) ? 2.0 : ((k != l) ? 2.0 : 1.0);
+                double f = ab_pair_data[ij] * cd_pair_data[kl] * cd_mat_D[kl] * w8;
+                for (int x = 0; x < 3; x++) {
+                    int ap[3] = {a[0], a[1], a[2]}, am[3] = {a[0], a[1], a[2]};
+                    int bp[3] = {b[0], b[1], b[2]}, bm[3] = {b[0], b[1], b[2]};
+                    ap[x] += 1; am[x] -= 1; bp[x] += 1; bm[x] -= 1;
+                    double dA = 2.0 * ai * quartet_component(c, ap, b, kc, kd);
+                    if (a[x] > 0) dA -= a[x] * quartet_component(c, am, b, kc, kd);
+                    double dB = 2.0 * aj * quartet_component(c, a, bp, kc, kd);
+                    if (b[x] > 0) dB -= b[x] * quartet_component(c, a, bm, kc, kd);
+                    g[x] += f * dA;
+                    g[3 + x] += f * dB;
+                }
+            }
+            for (int t = 0; t < 6; t++) grad_J[(uint64_t)t * gstride + ij] += g[t];
         }
         ctx_free(c);
     }

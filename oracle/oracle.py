@@ -48,6 +48,13 @@ def lib():
                _u32p, _u32p, _f64p, ctypes.c_uint32,
                ctypes.c_double, _u32p, ctypes.c_uint32]
         )
+        L.oracle_coulomb_grad.argtypes = (
+            [ctypes.c_int] * 4
+            + [_f64p, ctypes.c_uint64, ctypes.POINTER(_f64p), _u32p, _f64p, _f64p, _f64p,
+               _u32p, _u32p, _f64p, ctypes.c_uint32,
+               _u32p, _u32p, _f64p, ctypes.c_uint32,
+               ctypes.c_double, _u32p, ctypes.c_uint32]
+        )
         L.oracle_exchange_fock.argtypes = (
             [ctypes.c_int] * 4
             + [_f64p, _u32p, _u32p, ctypes.c_uint32,
@@ -159,6 +166,33 @@ def coulomb_fock(la, lb, lc, ld, prim_info, prim_count, cd_D, ab_Q, cd_Q,
         arrs[6][1], arrs[7][1], arrs[8][1], n_cd, float(thr), rp, nr)
     del keep, arrs, r
     return mat_J
+
+
+def coulomb_grad(la, lb, lc, ld, prim_info, prim_count, cd_D, ab_Q, cd_Q,
+                 ab_first, ab_second, ab_pdata, cd_first, cd_second, cd_pdata,
+                 thr, rows=None, grad=None):
+    """Oracle bra-centre derivatives of J for one class: array (6, n_ab),
+    rows 0..2 d mat_J / dA, rows 3..5 d mat_J / dB (+= onto grad)."""
+    n_ab = len(ab_first)
+    n_cd = len(cd_first)
+    if grad is None:
+        grad = np.zeros((6, n_ab))
+    grad = np.ascontiguousarray(grad, dtype=np.float64)
+    assert grad.shape == (6, n_ab)
+    infos, _, counts, keep = _prim_tables(prim_info, prim_count)
+    arrs = [_f(cd_D), _f(ab_Q), _f(cd_Q), _u(ab_first), _u(ab_second), _f(ab_pdata),
+            _u(cd_first), _u(cd_second), _f(cd_pdata)]
+    if rows is None:
+        r, rp, nr = None, None, 0
+    else:
+        r, rp = _u(rows)
+        nr = len(r)
+    lib().oracle_coulomb_grad(
+        la, lb, lc, ld, grad.ctypes.data_as(_f64p), n_ab, infos, counts.ctypes.data_as(_u32p),
+        arrs[0][1], arrs[1][1], arrs[2][1], arrs[3][1], arrs[4][1], arrs[5][1], n_ab,
+        arrs[6][1], arrs[7][1], arrs[8][1], n_cd, float(thr), rp, nr)
+    del keep, arrs, r
+    return grad
 
 
 def exchange_fock(la, lb, lc, ld, pair_i, pair_k, prim_info, prim_aoinds, prim_count,

@@ -51,6 +51,52 @@ def oracle_jk_all(rl: ReferenceLists, omega=0.0):
     return matJ, matK
 
 
+def bra_weights(rl: ReferenceLists, key: str) -> np.ndarray:
+    """w_o D_o of the entries of J list `key` (w_o = 1 on the diagonal of a
+    same-type list, else 2), so that 1/2 Tr[D J] = 1/2 sum_o w_o D_o mat_J[o]."""
+    jl = rl.jlists[key]
+    same = key[0] == key[1]
+    return np.where(same & (jl.first == jl.second), 1.0, 2.0) * jl.D
+
+
+def oracle_coulomb_energy(rl: ReferenceLists) -> float:
+    """E_J = 1/2 Tr[D J] from the oracle J of every class."""
+    from vlxb.lists import j_classes
+
+    E = 0.0
+    for cls in j_classes():
+        if cls[:2] in rl.jlists and cls[2:] in rl.jlists:
+            E += 0.5 * float(np.dot(bra_weights(rl, cls[:2]), oracle_J(rl, cls)))
+    return E
+
+
+def oracle_grad_class(rl: ReferenceLists, cls: str, grad=None):
+    a, b, c, d = cls
+    jab, jcd = rl.jlists[a + b], rl.jlists[c + d]
+    return oracle.coulomb_grad(LV[a], LV[b], LV[c], LV[d], rl.pd.info, rl.pd.count, jcd.D, jab.Q, jcd.Q,
+                               jab.first, jab.second, jab.pdata, jcd.first, jcd.second, jcd.pdata,
+                               rl.threshold, grad=grad)
+
+
+def oracle_coulomb_gradient(rl: ReferenceLists, natoms: int):
+    """dE_J/dR (natoms x 3) from the oracle's bra-centre derivatives of every
+    class, and the per-list derivative arrays (6, n) it was folded from."""
+    from vlxb.lists import NCART, j_classes
+
+    grads = {k: np.zeros((6, len(v.first))) for k, v in rl.jlists.items()}
+    for cls in j_classes():
+        if cls[:2] in rl.jlists and cls[2:] in rl.jlists:
+            oracle_grad_class(rl, cls, grad=grads[cls[:2]])
+    g = np.zeros((natoms, 3))
+    for k, G in grads.items():
+        jl = rl.jlists[k]
+        la, lb = LV[k[0]], LV[k[1]]
+        w = bra_weights(rl, k)
+        np.add.at(g, rl.pd.atom[la][jl.first // NCART[la]], (w * G[:3]).T)
+        np.add.at(g, rl.pd.atom[lb][jl.second // NCART[lb]], (w * G[3:]).T)
+    return g, grads
+
+
 def ao_eri_tensor(mol):
     """Full contracted Cartesian AO ERI tensor from the oracle (tiny systems only)."""
     from vlxb.basis import NCART

@@ -1,0 +1,100 @@
+"""GPU parity of the Coulomb nuclear gradient against the oracle.
+
+The oracle's gradient is pinned by finite differences of its J energy
+(test_gradient_oracle.py); here every vlxb_computeCoulombGradient<ABCD> entry
+point, called through the C ABI, is compared with the oracle's bra-centre
+derivatives of the same class, and the per-atom gradient with the oracle's.
+
+Tolerances (FP64): per class and per atom, max |GPU - oracle| <= 1e-10 *
+max |oracle| + 1e-14, the bar of the FP64 J build.  Mixed precision (FP32
+below a screening bound of 1e-6): max |dG| <= 1e-6 on gradients of order 1.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+import helpers
+from vlxb import basis, fock, gradient, lists
+from vlxb._lib import lib
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-10
+
+
+def close(got, exp):
+    scale = float(np.abs(exp).max()) if exp.size else 0.0
+    return float(np.abs(got - exp).max()) <= RTOL * scale + 1e-14 if exp.size else True
+
+
+@pytest.fixture(scope="module")
+def system():
+    lib().init(0)
+    wl = basis.config_custom(3, 4.0, {0: 2, 1: 1, 2: 1}, 2, 0.2, 2.5, 3, 1e-12, 29)
+    rl = lists.build_lists(wl.mol, wl.D, wl.threshold, fock.gpu_schwarz_fn())
+    g, grads = helpers.oracle_coulomb_gradient(rl, wl.mol.natoms)
+    return wl, rl, g, grads
+
+
+def test_every_gradient_class_vs_oracle(system):
+    wl, rl, _, _ = system
+    dl = fock.to_device(rl)
+    s = torch.cuda.current_stream().cuda_stream
+    bad = []
+    for cls in lists.j_classes():
+        n = len(rl.jlists[cls[:2]].first)
+        G = torch.zeros((6, n + 3), dtype=torch.float64, device="cuda")  # stride > count
+        lib().coulomb_grad(cls, gradient.grad_args(dl, cls, G, 0, n + 3, s))
+        got = G.cpu().numpy()
+        exp = helpers.oracle_grad_class(rl, cls)
+        if not close(got[:, :n], exp) or np.any(got[:, n:] != 0.0):
+            bad.append((cls, float(np.abs(got[:, :n] - exp).max())))
+    assert not bad, bad
+
+
+def test_atom_gradient_vs_oracle_and_invariance(system):
+    wl, rl, g_or, _ = system
+    dl = fock.to_device(rl)
+    cg = gradient.CoulombGradient(dl, wl.mol)
+    g1 = cg.compute().cpu().numpy()
+    g2 = cg.compute().cpu().numpy()
+    assert np.array_equal(g1, g2)  # fixed summation order: bit-reproducible
+    assert close(g1, g_or), float(np.abs(g1 - g_or).max())
+    assert np.abs(g1.sum(axis=0)).max() <= 1e-9 * max(1.0, np.abs(g1).max())
+
+
+def test_device_lists_gradient(system):
+    """The convenience call (lists built on the GPU) gives the host-list result."""
+    wl, _, g_or, _ = system
+    g = gradient.coulomb_gradient(wl.mol, wl.D, wl.threshold).cpu().numpy()
+    assert np.abs(g - g_or).max() <= 1e-10 * max(1.0, np.abs(g_or).max())
+
+
+def test_mixed_precision_gradient(system):
+    wl, rl, g_or, _ = system
+    dl = fock.to_device(rl)
+    L = lib()
+    try:
+        L.set_fp32_cut(1e-6)
+        g32 = gradient.CoulombGradient(dl, wl.mol).compute().cpu().numpy()
+    finally:
+        L.set_fp32_cut(0.0)
+    assert np.abs(g32 - g_or).max() <= 1e-6
+
+
+def test_gradient_argument_checks(system):
+    wl, rl, _, _ = system
+    dl = fock.to_device(rl)
+    s = torch.cuda.current_stream().cuda_stream
+    n = len(rl.jlists["pd"].first)
+    G = torch.zeros((6, n), dtype=torch.float64, device="cuda")
+    args = gradient.grad_args(dl, "pdpd", G, 0, n - 1, s)  # stride below the entry count
+    vals = [args[p] for p in L_params("pdpd")]
+    rc = getattr(lib().cdll, "vlxb_computeCoulombGradientPDPD")(*vals)
+    assert rc == 1  # VLXB_EINVAL
+    torch.cuda.synchronize()
+    assert float(G.abs().max()) == 0.0
+
+
+def L_params(cls):
+    return lib().g_params[cls]

@@ -106,7 +106,53 @@ energy_final_kernel(const double* __restrict__ part, int nblk, double* __restric
     }
 }
 
+// Nuclear gradient: one block per (atom, Cartesian direction) row; threads
+// take the atom's CSR entries in a fixed stride, then a fixed-order block sum.
+constexpr int GA_THREADS = 256;
+
+__global__ void __launch_bounds__(GA_THREADS)
+pair_grad_atoms_kernel(const double* __restrict__ pg, int64_t gs, const double* __restrict__ w,
+                       const int64_t* __restrict__ rowptr, const uint32_t* __restrict__ src,
+                       double* __restrict__ out)
+{
+    __shared__ double red[GA_THREADS / 32];
+    const int row = blockIdx.x;
+    const int t = row / 3, x = row % 3;
+    const int64_t e0 = __ldg(rowptr + t), e1 = __ldg(rowptr + t + 1);
+    double s = 0.0;
+    for (int64_t e = e0 + threadIdx.x; e < e1; e += GA_THREADS) {
+        const uint32_t v = __ldg(src + e);
+        const int64_t p = v & 0x7fffffffu;
+        const int64_t side = v >> 31;
+        s = fma(__ldg(w + p), __ldg(pg + (3 * side + x) * gs + p), s);
+    }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0;
+        for (int k = 0; k < GA_THREADS / 32; k++) a += red[k];
+        out[row] = a;
+    }
+}
+
 }  // namespace vlxb
+
+extern "C" int vlxb_pairGradientToAtoms(const double* pair_grad, uint64_t grad_stride, const double* weight,
+                                        const int64_t* rowptr, const uint32_t* src, int32_t n_atoms,
+                                        double* grad_atoms, void* stream)
+{
+    using namespace vlxb;
+    if (n_atoms <= 0 || !grad_atoms || !rowptr) return VLXB_EINVAL;
+    if (grad_stride > (uint64_t)INT64_MAX / 8 || (int64_t)n_atoms * 3 > (int64_t)INT32_MAX) return VLXB_EINVAL;
+    if (grad_stride > 0 && (!pair_grad || !weight || !src)) return VLXB_EINVAL;
+    cudaStream_t st = (cudaStream_t)stream;
+    pair_grad_atoms_kernel<<<3 * n_atoms, GA_THREADS, 0, st>>>(pair_grad, (int64_t)grad_stride, weight, rowptr,
+                                                               src, grad_atoms);
+    note_launches();
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    return VLXB_OK;
+}
 
 extern "C" int vlxb_pairsToAO(const double* pair_values, const int64_t* rowptr, const int32_t* row_ao,
                               const uint32_t* src, int64_t n_rows, double* mat_AO, int32_t naos, void* stream)

@@ -59,10 +59,12 @@ struct ExchangeArgs {
 };
 
 // Coulomb class call on a given arena (pool, static or measuring) with given
-// Boys tables and quartet counter (may be null).
-template <int LA, int LB, int LC, int LD>
+// Boys tables and quartet counter (may be null).  G = 1: the bra-centre
+// derivatives of J instead (coulomb_md_kernel<..., 1>), written to
+// a.mat_J[k * gstride + o], k = 0..5.
+template <int LA, int LB, int LC, int LD, int G = 0>
 int run_coulomb_impl(const CoulombArgs& a, cudaStream_t st, Arena& ar, const BoysTabs& tab,
-                     unsigned long long* qc, double cut)
+                     unsigned long long* qc, double cut, int64_t gstride = 0)
 {
     if (a.n_ab == 0 || a.n_cd == 0) return VLXB_OK;
     if (!a.mat_J || !a.cd_D || !a.ab_Q || !a.cd_Q || !a.ab_first || !a.ab_second || !a.ab_pdata || !a.cd_first ||
@@ -72,6 +74,7 @@ int run_coulomb_impl(const CoulombArgs& a, cudaStream_t st, Arena& ar, const Boy
     for (int t = 0; t < 4; t++)
         if (!a.info[L4[t]] || a.count[L4[t]] == 0) return VLXB_EINVAL;
     if (!(a.thr >= 0.0)) return VLXB_EINVAL;
+    if (G && gstride < (int64_t)a.n_ab) return VLXB_EINVAL;
     if (!tab.f64 || !tab.f32) return VLXB_ECUDA;
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     PairGroups gb, gk;
@@ -85,7 +88,7 @@ int run_coulomb_impl(const CoulombArgs& a, cudaStream_t st, Arena& ar, const Boy
     if (rc) return rc;
     const bool batched = a.prim_mol_a && a.prim_mol_c && a.n_mol > 0;
     JKetData kd;
-    const int jvar = schedule_get(0, LA, LB, LC, LD);
+    const int jvar = G ? 2 : schedule_get(0, LA, LB, LC, LD);
     rc = jket_prepare<LC, LD>(ar, gk, a.cd_first, a.cd_second, a.cd_D, a.cd_Q, a.cd_pdata, kd,
                               batched ? a.prim_mol_c : nullptr, batched ? a.n_mol : 0, jvar == 2);
     if (rc) return rc;
@@ -102,13 +105,20 @@ int run_coulomb_impl(const CoulombArgs& a, cudaStream_t st, Arena& ar, const Boy
     int grid = launch_grid_limit();
     if ((int64_t)grid > (int64_t)a.n_ab) grid = (int)a.n_ab;
     for (int pm = 0; pm < (cut > 0.0 ? 2 : 1); pm++) {
-        if (jvar == 2) {
+        if constexpr (G == 1) {
+            if (pm == 0)
+                coulomb_md_kernel<LA, LB, LC, LD, 0, 1><<<grid, MD_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab,
+                                                                                     nullptr, cut, gstride);
+            else
+                coulomb_md_kernel<LA, LB, LC, LD, 1, 1><<<grid, MD_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab,
+                                                                                     nullptr, cut, gstride);
+        } else if (jvar == 2) {
             if (pm == 0)
                 coulomb_md_kernel<LA, LB, LC, LD, 0><<<grid, MD_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc,
-                                                                                  cut);
+                                                                                  cut, 0);
             else
                 coulomb_md_kernel<LA, LB, LC, LD, 1><<<grid, MD_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc,
-                                                                                  cut);
+                                                                                  cut, 0);
         } else if (jvar == 1) {
             if (pm == 0)
                 coulomb_col_kernel<LA, LB, LC, LD, 0><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc,
@@ -138,6 +148,20 @@ int run_coulomb(const CoulombArgs& a, cudaStream_t st)
     if (!tab.f64 || !tab.f32) return VLXB_ECUDA;
     Arena ar(st);
     return run_coulomb_impl<LA, LB, LC, LD>(a, st, ar, tab, quartet_counters_device(), fp32_cut_get());
+}
+
+// Bra-centre derivatives of one Coulomb class: grad[k * gstride + o] +=
+// d mat_J[o] / d (A_x, A_y, A_z, B_x, B_y, B_z)[k], ket held fixed.
+template <int LA, int LB, int LC, int LD>
+int run_coulomb_grad(const CoulombArgs& a, int64_t gstride, cudaStream_t st)
+{
+    if (a.n_ab == 0 || a.n_cd == 0) return VLXB_OK;
+    int rc = ensure_pool_configured();
+    if (rc) return rc;
+    const BoysTabs tab{boys_table_device(), boys_table32_device()};
+    if (!tab.f64 || !tab.f32) return VLXB_ECUDA;
+    Arena ar(st);
+    return run_coulomb_impl<LA, LB, LC, LD, 1>(a, st, ar, tab, nullptr, fp32_cut_get(), gstride);
 }
 
 template <int LA, int LB, int LC, int LD>

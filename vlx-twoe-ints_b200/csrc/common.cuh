@@ -110,10 +110,11 @@ struct QVT {
 using QV = QVT<double>;
 
 // Primitive-pair geometry records (one per primitive shell pair), SoA in HBM.
-// Bra: zeta, 0.5/zeta, P[3], PA = P - A [3], AB = A - B [3].
-// Ket: eta,  0.5/eta,  Q[3], QC = Q - C [3], CD = C - D [3].
-constexpr int GEO_N = 11;
-enum GeoField { G_Z = 0, G_I2Z, G_PX, G_PY, G_PZ, G_AX, G_AY, G_AZ, G_RX, G_RY, G_RZ };
+// Bra: zeta, 0.5/zeta, P[3], PA = P - A [3], AB = A - B [3], alpha (A's exponent).
+// Ket: eta,  0.5/eta,  Q[3], QC = Q - C [3], CD = C - D [3], gamma (C's exponent).
+// The exponent row is read only by the gradient kernels.
+constexpr int GEO_N = 12;
+enum GeoField { G_Z = 0, G_I2Z, G_PX, G_PY, G_PZ, G_AX, G_AY, G_AZ, G_RX, G_RY, G_RZ, G_ALPHA };
 
 struct PairGeo {
     double z, i2z, Px, Py, Pz, Ax, Ay, Az, Rx, Ry, Rz;

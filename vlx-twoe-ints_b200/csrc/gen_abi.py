@@ -12,6 +12,8 @@ generator emits, so a caller that binds those kernels binds these instead:
   computeExchangeFock<ABCD>  gen_exchange.py:75-115 (identical in
                              new_exchange_code/exchangefockwriter.py:55-104),
                              classes new_exchange_code/gen_eri_exchange.py:39-56
+plus vlxb_computeCoulombGradient<ABCD> (bra-centre derivatives of J, the
+generator's unused gradient='a'/'b' terms, eri.py:85-129) with the J arguments.
 Each entry point takes one extra trailing argument, the CUDA stream (void*,
 NULL = default stream), and returns a status code instead of void.
 """
@@ -53,6 +55,12 @@ def j_params(cls):
           "const double* boys_func_table", "const double* boys_func_ft", "double eri_threshold",
           "void* stream"]
     return p
+
+
+def g_params(cls):
+    """Coulomb gradient: the J arguments with mat_J replaced by the derivative
+    output and its component stride."""
+    return ["double* grad_J", "uint64_t grad_stride"] + j_params(cls)[1:]
 
 
 def k_params(cls):
@@ -252,6 +260,35 @@ def header():
         L.append(f"/* replaces computeCoulombFock{cls.upper()} (gen_coulomb.py:74-93; class list gen_coulomb.py:47-56) */")
         L.append(f"int vlxb_computeCoulombFock{cls.upper()}(" + ", ".join(j_params(cls)) + ");")
     L.append("")
+    L += ["/* ---- Coulomb nuclear gradient ----",
+          "   vlxb_computeCoulombGradient<ABCD>: same arguments as",
+          "   vlxb_computeCoulombFock<ABCD> with mat_J replaced by grad_J, a",
+          "   [6][grad_stride] array (grad_stride >= ab_prim_pair_count_local):",
+          "   grad_J[k * grad_stride + o] += d mat_J[o] / d X_k for every bra list entry",
+          "   o, X = (A_x, A_y, A_z, B_x, B_y, B_z) the centres of the entry's first and",
+          "   second primitive, the ket pairs and cd_mat_D held fixed.  Derivative of",
+          "   a Cartesian Gaussian: d/dA_x phi_a = 2 alpha phi_{a+1x} - a_x phi_{a-1x}",
+          "   (the reference generator's gradient='a'/'b' terms, eri.py:85-129, which",
+          "   no reference generator emits).  Same screening (|Q_ij Q_kl D_kl| >",
+          "   eri_threshold), same mixed-precision cutoff as the J entry points.  For",
+          "   E_J = 1/2 Tr[D J] every J class's bra derivative weighted by",
+          "   w_o D_o (w_o = 1 for a diagonal entry of a same-type list, else 2) sums to",
+          "   dE_J/dR, the ket side being the same sum by symmetry.  No reference",
+          "   counterpart. */"]
+    for cls in j_classes():
+        L.append(f"int vlxb_computeCoulombGradient{cls.upper()}(" + ", ".join(g_params(cls)) + ");")
+    L += ["",
+          "/* Per-atom reduction of pair derivatives (after the gradient entry points):",
+          "   grad_atoms[3 * t + x] = sum over CSR entries e in rowptr[t] .. rowptr[t+1]-1",
+          "   of weight[p] * pair_grad[(3 * side + x) * grad_stride + p], with",
+          "   p = src[e] & 0x7fffffff and side = src[e] >> 31 (0: first centre, 1:",
+          "   second).  Overwrites grad_atoms (3 * n_atoms doubles).  Entries are",
+          "   summed in a fixed order: results are bit-reproducible.  No reference",
+          "   counterpart. */",
+          "int vlxb_pairGradientToAtoms(const double* pair_grad, uint64_t grad_stride, const double* weight,",
+          "                             const int64_t* rowptr, const uint32_t* src, int32_t n_atoms,",
+          "                             double* grad_atoms, void* stream);",
+          ""]
     L.append("/* ---- Exchange: replace computeExchangeFock<ABCD> of gen_exchange.py:75-115 ---- */")
     for cls in k_classes():
         L.append(f"/* replaces computeExchangeFock{cls.upper()} (gen_exchange.py:75-115; "
@@ -269,6 +306,8 @@ def abi_cu():
     for cls in j_classes():
         la, lb, lc, ld = (LV[x] for x in cls)
         L.append(f"int coulomb_{cls}(const CoulombArgs&, cudaStream_t);")
+    for cls in j_classes():
+        L.append(f"int coulomb_grad_{cls}(const CoulombArgs&, int64_t, cudaStream_t);")
     for cls in k_classes():
         L.append(f"int exchange_{cls}(const ExchangeArgs&, cudaStream_t);")
     L += ["}  // namespace vlxb", "", 'extern "C" {', ""]
@@ -290,6 +329,24 @@ def abi_cu():
               f"    A.cd_pdata = {c}{d}_pair_data; A.n_cd = {c}{d}_prim_pair_count;",
               "    A.thr = eri_threshold;",
               f"    return vlxb::coulomb_{cls}(A, (cudaStream_t)stream);", "}", ""]
+    for cls in j_classes():
+        a, b, c, d = cls
+        L.append(f"int vlxb_computeCoulombGradient{cls.upper()}(" + ", ".join(g_params(cls)) + ")")
+        L.append("{")
+        L.append("    (void)boys_func_table; (void)boys_func_ft;")
+        L.append("    if (grad_stride > (uint64_t)INT64_MAX) return VLXB_EINVAL;")
+        L.append("    vlxb::CoulombArgs A{};")
+        L.append("    A.mat_J = grad_J;")
+        for x in ANG:
+            if x in cls:
+                L.append(f"    A.info[{LV[x]}] = {x}_prim_info; A.count[{LV[x]}] = {x}_prim_count;")
+        L += [f"    A.cd_D = {c}{d}_mat_D; A.ab_Q = {a}{b}_mat_Q_local; A.cd_Q = {c}{d}_mat_Q;",
+              f"    A.ab_first = {a}{b}_first_inds_local; A.ab_second = {a}{b}_second_inds_local;",
+              f"    A.ab_pdata = {a}{b}_pair_data_local; A.n_ab = {a}{b}_prim_pair_count_local;",
+              f"    A.cd_first = {c}{d}_first_inds; A.cd_second = {c}{d}_second_inds;",
+              f"    A.cd_pdata = {c}{d}_pair_data; A.n_cd = {c}{d}_prim_pair_count;",
+              "    A.thr = eri_threshold;",
+              f"    return vlxb::coulomb_grad_{cls}(A, (int64_t)grad_stride, (cudaStream_t)stream);", "}", ""]
     for cls in k_classes():
         a, b, c, d = cls
         same = (c + d) == (a + b)
@@ -368,6 +425,8 @@ def class_tu(cls, kind):
     if kind == "j":
         L.append(f"int coulomb_{cls}(const CoulombArgs& a, cudaStream_t s) "
                  f"{{ return run_coulomb<{la}, {lb}, {lc}, {ld}>(a, s); }}")
+        L.append(f"int coulomb_grad_{cls}(const CoulombArgs& a, int64_t gs, cudaStream_t s) "
+                 f"{{ return run_coulomb_grad<{la}, {lb}, {lc}, {ld}>(a, gs, s); }}")
     else:
         L.append(f"int exchange_{cls}(const ExchangeArgs& a, cudaStream_t s) "
                  f"{{ return run_exchange<{la}, {lb}, {lc}, {ld}>(a, s); }}")

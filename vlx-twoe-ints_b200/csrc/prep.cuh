@@ -101,7 +101,8 @@ __global__ void k_scan_total(const int* __restrict__ scan, const int* __restrict
     if (blockIdx.x == 0 && threadIdx.x == 0) out[0] = (n > 0) ? scan[n - 1] + flag[n - 1] : 0;
 }
 
-// Pair geometry (see PairGeo): z, 0.5/z, P, P - A, A - B.
+// Pair geometry (see PairGeo): z, 0.5/z, P, P - A, A - B, and the first
+// centre's exponent.
 __global__ void k_pair_geo(const int* __restrict__ n_sp, const int32_t* __restrict__ sp_i,
                            const int32_t* __restrict__ sp_j, const double* __restrict__ info_a, uint32_t cnt_a,
                            const double* __restrict__ info_b, uint32_t cnt_b, double* __restrict__ geo,
@@ -116,6 +117,7 @@ __global__ void k_pair_geo(const int* __restrict__ n_sp, const int32_t* __restri
         const double z = ai + aj, iz = 1.0 / z;
         geo[G_Z * stride + s] = z;
         geo[G_I2Z * stride + s] = 0.5 * iz;
+        geo[G_ALPHA * stride + s] = ai;
 #pragma unroll
         for (int x = 0; x < 3; x++) {
             const double P = (ai * A[x] + aj * B[x]) * iz;

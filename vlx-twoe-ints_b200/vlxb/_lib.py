@@ -36,6 +36,8 @@ def _ctype(decl: str):
         return ctypes.c_void_p
     if t.endswith("uint32_t"):
         return ctypes.c_uint32
+    if t.endswith("uint64_t"):
+        return ctypes.c_uint64
     if t.endswith("double"):
         return ctypes.c_double
     if t.endswith("int"):
@@ -57,6 +59,13 @@ class Lib:
             f.argtypes = [_ctype(p) for p in ps]
             f.restype = ctypes.c_int
             self.j_params[cls] = [ABI.pname(p) for p in ps]
+        self.g_params = {}
+        for cls in ABI.j_classes():
+            ps = ABI.g_params(cls)
+            f = getattr(self.cdll, f"vlxb_computeCoulombGradient{cls.upper()}")
+            f.argtypes = [_ctype(p) for p in ps]
+            f.restype = ctypes.c_int
+            self.g_params[cls] = [ABI.pname(p) for p in ps]
         for cls in ABI.k_classes():
             ps = ABI.k_params(cls)
             f = getattr(self.cdll, f"vlxb_computeExchangeFock{cls.upper()}")
@@ -90,6 +99,8 @@ class Lib:
                                              ctypes.c_void_p]
         c.vlxb_blockMaxAbs.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int64,
                                        ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
+        c.vlxb_pairGradientToAtoms.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]
         for fn in (c.vlxb_coulombBatch, c.vlxb_exchangeBatch):
             fn.argtypes = [ctypes.c_int] * 4 + [ctypes.c_void_p, ctypes.c_void_p]
             fn.restype = ctypes.c_int
@@ -105,6 +116,11 @@ class Lib:
         vals = [args[n] for n in self.j_params[cls]]
         rc = getattr(self.cdll, f"vlxb_computeCoulombFock{cls.upper()}")(*vals)
         self.check(rc, f"vlxb_computeCoulombFock{cls.upper()}")
+
+    def coulomb_grad(self, cls: str, args: dict) -> None:
+        vals = [args[n] for n in self.g_params[cls]]
+        rc = getattr(self.cdll, f"vlxb_computeCoulombGradient{cls.upper()}")(*vals)
+        self.check(rc, f"vlxb_computeCoulombGradient{cls.upper()}")
 
     def exchange(self, cls: str, args: dict) -> None:
         vals = [args[n] for n in self.k_params[cls]]

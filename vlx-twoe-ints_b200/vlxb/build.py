@@ -52,7 +52,8 @@ def _deps(src):
     base = os.path.basename(src)
     if base.startswith("cls_"):
         deps.append(os.path.join(GEN, f"col_{base.split('_')[1]}.cuh"))
-        deps.append(os.path.join(GEN, f"q_{base.split('_')[1]}.cuh"))
+        with open(src) as fh:  # every generated quartet header the unit includes (its class first)
+            deps += [os.path.join(GEN, ln.split('"')[1]) for ln in fh if ln.startswith('#include "q_')]
     if base == "prep.cu":
         deps.append(os.path.join(GEN, "schedule_default.inc"))
     return deps
@@ -89,7 +90,7 @@ def build(jobs: int | None = None, verbose: bool = False) -> str:
     srcs = _sources()
     todo = [s for s in srcs if _stale(_obj(s), _deps(s))]
     # heaviest units first (d-rich classes) for a shorter critical path
-    todo.sort(key=lambda s: -os.path.getsize(_deps(s)[-1]) if os.path.basename(s).startswith("cls_") else 0)
+    todo.sort(key=lambda s: -sum(os.path.getsize(d) for d in _deps(s) if os.path.basename(d).startswith("q_")))
     jobs = jobs or max(1, os.cpu_count() or 1)
     if todo:
         with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
