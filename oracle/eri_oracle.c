@@ -19,9 +19,10 @@
  *   - Range separation: d2 = w^2/(rho + w^2), Lambda *= sqrt(d2),
  *     T *= d2, F_m *= d2^m: gen_exchange.py:278-298.
  *   - J digestion with the k<->l doubling weights: gen_coulomb.py:205-297.
- *   - Bra-centre derivatives of J (Coulomb nuclear gradient) by the
- *     Obara-Saika derivative relation, the generator's gradient='a' / 'b'
- *     terms (eri.py:85-129), on the same integrals and digestion.
+ *   - Bra-centre derivatives of J and the energy-weighted centre derivatives
+ *     of K (nuclear gradient) by the Obara-Saika derivative relation, the
+ *     generator's gradient='a' / 'b' / 'c' terms (eri.py:85-152), on the same
+ *     integrals, digestion and screening.
  *   - K digestion over partner lists with the max-D screen and the AO-density
  *     gather: gen_exchange.py:139-342.
  * Screening follows the set semantics that the reference's per-thread
@@ -427,6 +428,85 @@ void oracle_exchange_fock(int la, int lb, int lc, int ld, double* mat_K,
                 }
             }
             mat_K[ik] += K;
+        }
+        ctx_free(c);
+    }
+}
+
+/* Energy-weighted centre derivatives of K for one (ab|cd) class, per (i, k)
+   list entry (the exchange gradient):
+     grad[x * gstride + ik]     += w_ik D_ik sum_jl D_jl d(ij|kl)/dA_x,
+     grad[(3+x) * gstride + ik] += w_ik D_ik sum_jl D_jl d(ij|kl)/dC_x,
+   A, C the centres of i and k, w_ik = 1 for i == k of a same-type list, else
+   2, D_ik and D_jl read from the AO density as in oracle_exchange_fock, by the
+   Obara-Saika derivative relation (eri.py:85-152, the generator's gradient='a'
+   / 'c' terms).  Same partner loops and screening as oracle_exchange_fock. */
+void oracle_exchange_grad(int la, int lb, int lc, int ld, double* grad, uint64_t gstride,
+                          const uint32_t* pair_i, const uint32_t* pair_k, uint32_t n_ik,
+                          const double* const* prim_info, const uint32_t* const* prim_aoinds,
+                          const uint32_t* prim_count,
+                          double bd_max_D, const double* D_AO, uint32_t naos,
+                          const double* Q_ab, const double* Q_cd,
+                          const uint32_t* Dinds_ab, const uint32_t* Dinds_cd,
+                          const uint32_t* displs_ab, const uint32_t* displs_cd,
+                          const uint32_t* counts_ab, const uint32_t* counts_cd,
+                          const double* pdata_ab, const double* pdata_cd,
+                          double omega, double thr, const uint32_t* rows, uint32_t nrows)
+{
+    uint32_t nwork = rows ? nrows : n_ik;
+    int L = la + lb + lc + ld + 1;
+    int nca = ncart_of[la], ncb = ncart_of[lb], ncc = ncart_of[lc], ncd = ncart_of[ld];
+    #pragma omp parallel
+    {
+        OrCtx* c = ctx_new_nb(OR_MAXL + 2);
+        #pragma omp for schedule(dynamic, 1)
+        for (int64_t w = 0; w < (int64_t)nwork; w++) {
+            uint32_t ik = rows ? rows[w] : (uint32_t)w;
+            uint32_t i = pair_i[ik], k = pair_k[ik];
+            double ai, ak, ri[3], rk[3];
+            int ca, cc;
+            prim_of(prim_info[la], prim_count[la], la, i, &ai, ri, &ca);
+            prim_of(prim_info[lc], prim_count[lc], lc, k, &ak, rk, &cc);
+            uint32_t iao = prim_aoinds[la][i / (uint32_t)nca + prim_count[la] * (i % (uint32_t)nca)];
+            uint32_t kao = prim_aoinds[lc][k / (uint32_t)ncc + prim_count[lc] * (k % (uint32_t)ncc)];
+            double wik = ((la == lc) && (i == k) ? 1.0 : 2.0) * D_AO[(size_t)iao * naos + kao];
+            const int* a = cart_comp(la, ca);
+            const int* kc = cart_comp(lc, cc);
+            double g[6] = {0, 0, 0, 0, 0, 0};
+            for (uint32_t j = 0; j < counts_ab[i]; j++) {
+                uint32_t pj = displs_ab[i] + j;
+                double Qij = Q_ab[pj];
+                uint32_t jp = Dinds_ab[pj];
+                double aj, rj[3];
+                int cb;
+                prim_of(prim_info[lb], prim_count[lb], lb, jp, &aj, rj, &cb);
+                uint32_t jao = prim_aoinds[lb][jp / (uint32_t)ncb + prim_count[lb] * (jp % (uint32_t)ncb)];
+                const int* b = cart_comp(lb, cb);
+                for (uint32_t l = 0; l < counts_cd[k]; l++) {
+                    uint32_t pl = displs_cd[k] + l;
+                    if (fabs(Qij * Q_cd[pl] * bd_max_D) <= thr) continue;
+                    uint32_t lp = Dinds_cd[pl];
+                    double al, rl[3];
+                    int cd;
+                    prim_of(prim_info[ld], prim_count[ld], ld, lp, &al, rl, &cd);
+                    uint32_t lao = prim_aoinds[ld][lp / (uint32_t)ncd + prim_count[ld] * (lp % (uint32_t)ncd)];
+                    const int* d = cart_comp(ld, cd);
+                    setup_quartet(c, L, ai, ri, aj, rj, ak, rk, al, rl, omega);
+                    double f = pdata_ab[pj] * pdata_cd[pl] * D_AO[(size_t)jao * naos + lao];
+                    for (int x = 0; x < 3; x++) {
+                        int ap[3] = {a[0], a[1], a[2]}, am[3] = {a[0], a[1], a[2]};
+                        int cp[3] = {kc[0], kc[1], kc[2]}, cm[3] = {kc[0], kc[1], kc[2]};
+                        ap[x] += 1; am[x] -= 1; cp[x] += 1; cm[x] -= 1;
+                        double dA = 2.0 * ai * quartet_component(c, ap, b, kc, d);
+                        if (a[x] > 0) dA -= a[x] * quartet_component(c, am, b, kc, d);
+                        double dC = 2.0 * ak * quartet_component(c, a, b, cp, d);
+                        if (kc[x] > 0) dC -= kc[x] * quartet_component(c, a, b, cm, d);
+                        g[x] += f * dA;
+                        g[3 + x] += f * dC;
+                    }
+                }
+            }
+            for (int t = 0; t < 6; t++) grad[(uint64_t)t * gstride + ik] += wik * g[t];
         }
         ctx_free(c);
     }

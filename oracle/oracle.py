@@ -63,6 +63,14 @@ def lib():
                _f64p, _f64p, _u32p, _u32p, _u32p, _u32p, _u32p, _u32p, _f64p, _f64p,
                ctypes.c_double, ctypes.c_double, _u32p, ctypes.c_uint32]
         )
+        L.oracle_exchange_grad.argtypes = (
+            [ctypes.c_int] * 4
+            + [_f64p, ctypes.c_uint64, _u32p, _u32p, ctypes.c_uint32,
+               ctypes.POINTER(_f64p), ctypes.POINTER(_u32p), _u32p,
+               ctypes.c_double, _f64p, ctypes.c_uint32,
+               _f64p, _f64p, _u32p, _u32p, _u32p, _u32p, _u32p, _u32p, _f64p, _f64p,
+               ctypes.c_double, ctypes.c_double, _u32p, ctypes.c_uint32]
+        )
         L.oracle_num_threads.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -220,3 +228,32 @@ def exchange_fock(la, lb, lc, ld, pair_i, pair_k, prim_info, prim_aoinds, prim_c
         arrs[9][1], arrs[10][1], arrs[11][1], arrs[12][1], float(omega), float(thr), rp, nr)
     del keep, arrs, r
     return mat_K
+
+
+def exchange_grad(la, lb, lc, ld, pair_i, pair_k, prim_info, prim_aoinds, prim_count,
+                  bd_max_D, D_AO, Q_ab, Q_cd, Dinds_ab, Dinds_cd, displs_ab, displs_cd,
+                  counts_ab, counts_cd, pdata_ab, pdata_cd, omega, thr, rows=None, grad=None):
+    """Oracle energy-weighted centre derivatives of K for one class, per (i, k)
+    entry: array (6, n_ik), rows 0..2 for i's centre, 3..5 for k's (+= onto grad)."""
+    n_ik = len(pair_i)
+    if grad is None:
+        grad = np.zeros((6, n_ik))
+    grad = np.ascontiguousarray(grad, dtype=np.float64)
+    assert grad.shape == (6, n_ik)
+    infos, aoinds, counts, keep = _prim_tables(prim_info, prim_count, prim_aoinds)
+    D_AO = np.ascontiguousarray(D_AO, dtype=np.float64)
+    naos = D_AO.shape[0]
+    arrs = [_u(pair_i), _u(pair_k), _f(D_AO), _f(Q_ab), _f(Q_cd), _u(Dinds_ab), _u(Dinds_cd),
+            _u(displs_ab), _u(displs_cd), _u(counts_ab), _u(counts_cd), _f(pdata_ab), _f(pdata_cd)]
+    if rows is None:
+        r, rp, nr = None, None, 0
+    else:
+        r, rp = _u(rows)
+        nr = len(r)
+    lib().oracle_exchange_grad(
+        la, lb, lc, ld, grad.ctypes.data_as(_f64p), n_ik, arrs[0][1], arrs[1][1], n_ik,
+        infos, aoinds, counts.ctypes.data_as(_u32p), float(bd_max_D), arrs[2][1], naos,
+        arrs[3][1], arrs[4][1], arrs[5][1], arrs[6][1], arrs[7][1], arrs[8][1],
+        arrs[9][1], arrs[10][1], arrs[11][1], arrs[12][1], float(omega), float(thr), rp, nr)
+    del keep, arrs, r
+    return grad

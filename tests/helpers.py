@@ -97,6 +97,75 @@ def oracle_coulomb_gradient(rl: ReferenceLists, natoms: int):
     return g, grads
 
 
+def k_weights(rl: ReferenceLists, key: str) -> np.ndarray:
+    """w_ik D_ik of the entries of K (i, k) list `key`, so that
+    1/2 Tr[D K] = 1/2 sum_ik w_ik D_ik mat_K[ik]."""
+    from vlxb.lists import NCART
+
+    kp = rl.kpairs[key]
+    la, lc = LV[key[0]], LV[key[1]]
+    ai = rl.pd.aoinds[la][kp.pair_i % NCART[la], kp.pair_i // NCART[la]]
+    ck = rl.pd.aoinds[lc][kp.pair_k % NCART[lc], kp.pair_k // NCART[lc]]
+    w = np.where((la == lc) & (kp.pair_i == kp.pair_k), 1.0, 2.0)
+    return w * rl.D_AO[ai, ck]
+
+
+def oracle_exchange_energy(rl: ReferenceLists, omega=0.0) -> float:
+    """E_K = 1/2 Tr[D K] from the oracle K of every class."""
+    from vlxb.lists import k_classes
+
+    E = 0.0
+    for cls in k_classes():
+        ac = cls[0] + cls[2]
+        if ac in rl.kpairs and cls[:2] in rl.kpartners and cls[2:] in rl.kpartners:
+            E += 0.5 * float(np.dot(k_weights(rl, ac), oracle_K(rl, cls, omega)))
+    return E
+
+
+def oracle_kgrad_class(rl: ReferenceLists, cls: str, omega=0.0, grad=None):
+    a, b, c, d = cls
+    kq = rl.kpairs[a + c]
+    p1, p2 = rl.kpartners[a + b], rl.kpartners[c + d]
+    return oracle.exchange_grad(LV[a], LV[b], LV[c], LV[d], kq.pair_i, kq.pair_k, rl.pd.info, rl.pd.aoinds,
+                                rl.pd.count, rl.maxD[b + d], rl.D_AO, p1.Q, p2.Q, p1.Dinds, p2.Dinds, p1.displs,
+                                p2.displs, p1.counts, p2.counts, p1.pdata, p2.pdata, omega, rl.threshold, grad=grad)
+
+
+def oracle_exchange_gradient(rl: ReferenceLists, natoms: int, omega=0.0):
+    """dE_K/dR (natoms x 3) for E_K = 1/2 Tr[D K], and the per-list (6, n_ik)
+    arrays of per-entry values it was folded from."""
+    from vlxb.lists import NCART, k_classes
+
+    grads = {k: np.zeros((6, len(v.pair_i))) for k, v in rl.kpairs.items()}
+    for cls in k_classes():
+        ac = cls[0] + cls[2]
+        if ac in rl.kpairs and cls[:2] in rl.kpartners and cls[2:] in rl.kpartners:
+            oracle_kgrad_class(rl, cls, omega, grad=grads[ac])
+    g = np.zeros((natoms, 3))
+    for k, G in grads.items():
+        kp = rl.kpairs[k]
+        la, lc = LV[k[0]], LV[k[1]]
+        np.add.at(g, rl.pd.atom[la][kp.pair_i // NCART[la]], G[:3].T)
+        np.add.at(g, rl.pd.atom[lc][kp.pair_k // NCART[lc]], G[3:].T)
+    return g, grads
+
+
+def kgrad_blocks(rl: ReferenceLists, key: str, G: np.ndarray) -> np.ndarray:
+    """Per-entry K-gradient values summed onto each primitive shell block's
+    lowest list position (the layout of vlxb_computeExchangeGradient)."""
+    from vlxb.lists import NCART
+
+    kp = rl.kpairs[key]
+    la, lc = LV[key[0]], LV[key[1]]
+    blk = (kp.pair_i // NCART[la]).astype(np.int64) * (1 << 32) + kp.pair_k // NCART[lc]
+    out = np.zeros_like(G)
+    first = {}
+    for p, bk in enumerate(blk):
+        q = first.setdefault(int(bk), p)
+        out[:, q] += G[:, p]
+    return out
+
+
 def ao_eri_tensor(mol):
     """Full contracted Cartesian AO ERI tensor from the oracle (tiny systems only)."""
     from vlxb.basis import NCART

@@ -1,9 +1,10 @@
-"""GPU parity of the Coulomb nuclear gradient against the oracle.
+"""GPU parity of the Coulomb and exchange nuclear gradients against the oracle.
 
-The oracle's gradient is pinned by finite differences of its J energy
-(test_gradient_oracle.py); here every vlxb_computeCoulombGradient<ABCD> entry
-point, called through the C ABI, is compared with the oracle's bra-centre
-derivatives of the same class, and the per-atom gradient with the oracle's.
+The oracle's gradients are pinned by finite differences of its J and K
+energies (test_gradient_oracle.py); here every
+vlxb_computeCoulombGradient<ABCD> and vlxb_computeExchangeGradient<ABCD> entry
+point, called through the C ABI, is compared with the oracle's derivatives of
+the same class, and the per-atom gradients with the oracle's.
 
 Tolerances (FP64): per class and per atom, max |GPU - oracle| <= 1e-10 *
 max |oracle| + 1e-14, the bar of the FP64 J build.  Mixed precision (FP32
@@ -34,6 +35,12 @@ def system():
     rl = lists.build_lists(wl.mol, wl.D, wl.threshold, fock.gpu_schwarz_fn())
     g, grads = helpers.oracle_coulomb_gradient(rl, wl.mol.natoms)
     return wl, rl, g, grads
+
+
+@pytest.fixture(scope="module")
+def kref(system):
+    wl, rl, _, _ = system
+    return helpers.oracle_exchange_gradient(rl, wl.mol.natoms)
 
 
 def test_every_gradient_class_vs_oracle(system):
@@ -98,3 +105,48 @@ def test_gradient_argument_checks(system):
 
 def L_params(cls):
     return lib().g_params[cls]
+
+
+def test_every_exchange_gradient_class_vs_oracle(system):
+    """Each class's block values (at the block's lowest list position, nothing
+    elsewhere) against the oracle's per-entry values summed per block."""
+    wl, rl, _, _ = system
+    dl = fock.to_device(rl)
+    s = torch.cuda.current_stream().cuda_stream
+    bad = []
+    for cls in lists.k_classes():
+        ac = cls[0] + cls[2]
+        n = len(rl.kpairs[ac].pair_i)
+        G = torch.zeros((6, n + 5), dtype=torch.float64, device="cuda")
+        lib().exchange_grad(cls, gradient.kgrad_args(dl, cls, G, 0, n + 5, s))
+        got = G.cpu().numpy()
+        exp = helpers.kgrad_blocks(rl, ac, helpers.oracle_kgrad_class(rl, cls))
+        if not close(got[:, :n], exp) or np.any(got[:, n:] != 0.0) or np.any(got[:, :n][exp == 0.0] != 0.0):
+            bad.append((cls, float(np.abs(got[:, :n] - exp).max())))
+    assert not bad, bad
+
+
+def test_exchange_atom_gradient_vs_oracle(system, kref):
+    wl, rl, _, _ = system
+    g_or, _ = kref
+    dl = fock.to_device(rl)
+    eg = gradient.ExchangeGradient(dl, wl.mol)
+    g1 = eg.compute().cpu().numpy()
+    g2 = eg.compute().cpu().numpy()
+    assert np.array_equal(g1, g2)
+    assert close(g1, g_or), float(np.abs(g1 - g_or).max())
+    assert np.abs(g1.sum(axis=0)).max() <= 1e-9 * max(1.0, np.abs(g1).max())
+
+
+def test_range_separated_exchange_gradient(system):
+    wl, rl, _, _ = system
+    g_or, _ = helpers.oracle_exchange_gradient(rl, wl.mol.natoms, omega=0.4)
+    g = gradient.ExchangeGradient(fock.to_device(rl), wl.mol).compute(omega=0.4).cpu().numpy()
+    assert close(g, g_or), float(np.abs(g - g_or).max())
+
+
+def test_device_lists_exchange_gradient(system, kref):
+    wl, _, _, _ = system
+    g_or, _ = kref
+    g = gradient.exchange_gradient(wl.mol, wl.D, wl.threshold).cpu().numpy()
+    assert np.abs(g - g_or).max() <= 1e-10 * max(1.0, np.abs(g_or).max())

@@ -1,6 +1,7 @@
-"""Coulomb nuclear gradient: the oracle's bra-centre derivatives, pinned by
-central finite differences of the oracle's own J energy (itself pinned by the
-reference-generated golden vectors), and the host-side folding rules.
+"""Nuclear gradients of E_J = 1/2 Tr[D J] and E_K = 1/2 Tr[D K]: the oracle's
+derivative integrals, pinned by central finite differences of the oracle's
+own J and K energies (themselves pinned by the reference-generated golden
+vectors), and the host-side folding rules.
 
 System: three atoms at a bent geometry with one s, p and d shell each (one
 primitive), threshold 0, so that every pair is in every list and the energy
@@ -80,3 +81,27 @@ def test_derivative_sides_sum_to_product_derivative():
     # the bra side, which must cancel the ket side: total sum zero
     tot = (w * (G[:3] + G[3:])).sum(axis=1)
     assert np.abs(tot).max() <= 1e-12 * max(1.0, np.abs(G).max())
+
+
+def test_oracle_exchange_gradient_matches_finite_differences():
+    """dE_K/dR for E_K = 1/2 Tr[D K] against central differences of the
+    oracle's K energy (threshold 0)."""
+    mol, D = _system()
+    g, _ = helpers.oracle_exchange_gradient(_lists(mol, D), mol.natoms)
+    assert np.abs(g).max() > 1e-3
+    assert np.abs(g.sum(axis=0)).max() <= 1e-11 * max(1.0, np.abs(g).max())
+    for atom, x in ((1, 0), (2, 1), (2, 2)):
+        ep = helpers.oracle_exchange_energy(_lists(_moved(mol, atom, x, H), D))
+        em = helpers.oracle_exchange_energy(_lists(_moved(mol, atom, x, -H), D))
+        fd = (ep - em) / (2 * H)
+        assert abs(fd - g[atom, x]) <= FD_TOL, (atom, x, fd, g[atom, x])
+
+
+def test_oracle_range_separated_exchange_gradient():
+    """The same with the erf-attenuated operator (omega = 0.4)."""
+    mol, D = _system()
+    om = 0.4
+    g, _ = helpers.oracle_exchange_gradient(_lists(mol, D), mol.natoms, omega=om)
+    ep = helpers.oracle_exchange_energy(_lists(_moved(mol, 1, 1, H), D), omega=om)
+    em = helpers.oracle_exchange_energy(_lists(_moved(mol, 1, 1, -H), D), omega=om)
+    assert abs((ep - em) / (2 * H) - g[1, 1]) <= FD_TOL

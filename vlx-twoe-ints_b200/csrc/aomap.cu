@@ -124,7 +124,7 @@ pair_grad_atoms_kernel(const double* __restrict__ pg, int64_t gs, const double* 
         const uint32_t v = __ldg(src + e);
         const int64_t p = v & 0x7fffffffu;
         const int64_t side = v >> 31;
-        s = fma(__ldg(w + p), __ldg(pg + (3 * side + x) * gs + p), s);
+        s = fma(w ? __ldg(w + p) : 1.0, __ldg(pg + (3 * side + x) * gs + p), s);
     }
     s = warp_sum(s);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -145,7 +145,7 @@ extern "C" int vlxb_pairGradientToAtoms(const double* pair_grad, uint64_t grad_s
     using namespace vlxb;
     if (n_atoms <= 0 || !grad_atoms || !rowptr) return VLXB_EINVAL;
     if (grad_stride > (uint64_t)INT64_MAX / 8 || (int64_t)n_atoms * 3 > (int64_t)INT32_MAX) return VLXB_EINVAL;
-    if (grad_stride > 0 && (!pair_grad || !weight || !src)) return VLXB_EINVAL;
+    if (grad_stride > 0 && (!pair_grad || !src)) return VLXB_EINVAL;
     cudaStream_t st = (cudaStream_t)stream;
     pair_grad_atoms_kernel<<<3 * n_atoms, GA_THREADS, 0, st>>>(pair_grad, (int64_t)grad_stride, weight, rowptr,
                                                                src, grad_atoms);

@@ -5,6 +5,7 @@
 #include "engine.cuh"
 #include "jk_kernels.cuh"
 #include "md_kernels.cuh"
+#include "kgrad_kernels.cuh"
 
 namespace vlxb {
 
@@ -294,6 +295,68 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
         }
         note_launches();
     }
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    return VLXB_OK;
+}
+
+// Energy-weighted centre derivatives of one exchange class (see
+// exchange_grad_kernel): grad[x * gstride + p] += ..., p the lowest (i, k)
+// list position of each primitive shell block.  FP64, single-molecule calls.
+template <int LA, int LB, int LC, int LD>
+int run_exchange_grad(const ExchangeArgs& a, int64_t gstride, cudaStream_t st)
+{
+    if (a.n_ik == 0) return VLXB_OK;
+    if (!a.mat_K || !a.pair_i || !a.pair_k || !a.D || !a.Q_ab || !a.Q_cd || !a.Dinds_ab || !a.Dinds_cd ||
+        !a.displs_ab || !a.displs_cd || !a.counts_ab || !a.counts_cd || !a.pdata_ab || !a.pdata_cd || a.naos == 0)
+        return VLXB_EINVAL;
+    const int L4[4] = {LA, LB, LC, LD};
+    for (int t = 0; t < 4; t++)
+        if (!a.info[L4[t]] || !a.aoinds[L4[t]] || a.count[L4[t]] == 0) return VLXB_EINVAL;
+    if (!(a.thr >= 0.0) || !(a.omega >= 0.0)) return VLXB_EINVAL;
+    if (gstride < (int64_t)a.n_ik) return VLXB_EINVAL;
+    int rc = ensure_pool_configured();
+    if (rc) return rc;
+    const BoysTabs tab{boys_table_device(), boys_table32_device()};
+    if (!tab.f64) return VLXB_ECUDA;
+    constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    Arena ar(st);
+    KOutData ko;
+    rc = kout_prepare(ar, NA, NC, (int)a.count[LA], (int)a.count[LC], a.pair_i, a.pair_k, a.n_ik, ko);
+    if (rc) return rc;
+    const int npa = (int)a.count[LA], npb = (int)a.count[LB], npc = (int)a.count[LC], npd = (int)a.count[LD];
+    PairGroups gab;
+    rc = group_csr(ar, NA, NB, npa, npb, a.displs_ab, a.counts_ab, a.Dinds_ab, (int64_t)npa * npb, a.info[LA],
+                   a.count[LA], a.info[LB], a.count[LB], gab);
+    if (rc) return rc;
+    rc = make_records(ar, NA * NB, gab, a.Q_ab, (int64_t)npa * npb * NA * NB);
+    if (rc) return rc;
+    rc = segment_records(ar, NA * NB, npa, npb, gab, a.pdata_ab);
+    if (rc) return rc;
+    PairGroups gcd;
+    const bool same = (LA == LC && LB == LD && a.Q_ab == a.Q_cd && a.Dinds_ab == a.Dinds_cd &&
+                       a.displs_ab == a.displs_cd && a.counts_ab == a.counts_cd && a.pdata_ab == a.pdata_cd);
+    if (same) {
+        gcd = gab;
+    } else {
+        rc = group_csr(ar, NC, ND, npc, npd, a.displs_cd, a.counts_cd, a.Dinds_cd, (int64_t)npc * npd, a.info[LC],
+                       a.count[LC], a.info[LD], a.count[LD], gcd);
+        if (rc) return rc;
+        rc = make_records(ar, NC * ND, gcd, a.Q_cd, (int64_t)npc * npd * NC * ND);
+        if (rc) return rc;
+        rc = segment_records(ar, NC * ND, npc, npd, gcd, a.pdata_cd);
+        if (rc) return rc;
+    }
+    if (ar.failed()) return VLXB_ENOMEM;
+    KOutBlocks out{ko.ish, ko.ksh, ko.idx, ko.stride, ko.n, nullptr};
+    KPartnerRecs rab{gab.rec_sp, gab.rec_q, gab.rec_mask, gab.seg, gab.geo, gab.S, gab.sp_j, gab.sp_stride, gab.su};
+    KPartnerRecs rcd{gcd.rec_sp, gcd.rec_q, gcd.rec_mask, gcd.seg, gcd.geo, gcd.S, gcd.sp_j, gcd.sp_stride, gcd.su};
+    const KDensity dm{a.aoinds[LB], a.count[LB], a.aoinds[LD], a.count[LD], a.D, a.naos};
+    const KGradBlockD bd{a.aoinds[LA], a.count[LA], a.aoinds[LC], a.count[LC], LA == LC ? 1 : 0};
+    int grid = launch_grid_limit();
+    if ((int64_t)grid > (int64_t)a.n_ik) grid = (int)a.n_ik;
+    exchange_grad_kernel<LA, LB, LC, LD><<<grid, KGradShape<LA, LB, LC, LD>::THREADS, 0, st>>>(
+        out, rab, rcd, dm, bd, a.maxD, a.omega, a.thr, a.mat_K, gstride, tab);
+    note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
 }

@@ -13,7 +13,9 @@ generator emits, so a caller that binds those kernels binds these instead:
                              new_exchange_code/exchangefockwriter.py:55-104),
                              classes new_exchange_code/gen_eri_exchange.py:39-56
 plus vlxb_computeCoulombGradient<ABCD> (bra-centre derivatives of J, the
-generator's unused gradient='a'/'b' terms, eri.py:85-129) with the J arguments.
+generator's unused gradient='a'/'b' terms, eri.py:85-129) with the J arguments
+and vlxb_computeExchangeGradient<ABCD> (energy-weighted centre derivatives of K,
+gradient='a'/'c', eri.py:85-152, McMurchie-Davidson form) with the K arguments.
 Each entry point takes one extra trailing argument, the CUDA stream (void*,
 NULL = default stream), and returns a status code instead of void.
 """
@@ -80,6 +82,12 @@ def k_params(cls):
     p += ["const double* boys_func_table", "const double* boys_func_ft", "double omega", "double eri_threshold",
           "void* stream"]
     return p
+
+
+def kg_params(cls):
+    """Exchange gradient: the K arguments with mat_K replaced by the derivative
+    output and its component stride."""
+    return ["double* grad_K", "uint64_t grad_stride"] + k_params(cls)[1:]
 
 
 def pname(p):
@@ -281,14 +289,36 @@ def header():
           "/* Per-atom reduction of pair derivatives (after the gradient entry points):",
           "   grad_atoms[3 * t + x] = sum over CSR entries e in rowptr[t] .. rowptr[t+1]-1",
           "   of weight[p] * pair_grad[(3 * side + x) * grad_stride + p], with",
-          "   p = src[e] & 0x7fffffff and side = src[e] >> 31 (0: first centre, 1:",
-          "   second).  Overwrites grad_atoms (3 * n_atoms doubles).  Entries are",
+          "   p = src[e] & 0x7fffffff (< grad_stride) and side = src[e] >> 31 (0:",
+          "   first centre, 1: second); weight NULL = 1 (the exchange gradient comes",
+          "   weighted).  Overwrites grad_atoms (3 * n_atoms doubles).  Entries are",
           "   summed in a fixed order: results are bit-reproducible.  No reference",
           "   counterpart. */",
           "int vlxb_pairGradientToAtoms(const double* pair_grad, uint64_t grad_stride, const double* weight,",
           "                             const int64_t* rowptr, const uint32_t* src, int32_t n_atoms,",
           "                             double* grad_atoms, void* stream);",
           ""]
+    L += ["/* ---- Exchange nuclear gradient ----",
+          "   vlxb_computeExchangeGradient<ABCD>: same arguments as",
+          "   vlxb_computeExchangeFock<ABCD> with mat_K replaced by grad_K, a",
+          "   [6][grad_stride] array (grad_stride >= pair_inds_count_for_K_ac).  For",
+          "   every primitive shell block (i / ncart_a, k / ncart_c) of the (i, k) list",
+          "   it adds, at the block's lowest list position p,",
+          "     grad_K[x * grad_stride + p] += sum over the block's entries (i, k) of",
+          "       w_ik D_ik sum_jl D_jl d(ij|kl)/dX_x,",
+          "   X = (A_x, A_y, A_z, C_x, C_y, C_z) the centres of i and k, D the AO",
+          "   density (D_ik = mat_D_full_AO[ao(i)][ao(k)]), w_ik = 1 for i == k of a",
+          "   same-type list, else 2; the block's other positions receive nothing.",
+          "   Summed over the 54 classes and credited to the atoms of i (x < 3) and",
+          "   k (x >= 3) this is dE_K/dR for E_K = 1/2 Tr[D K] (the j and l centres",
+          "   are covered by the symmetry of the sum).  Same screening and omega as",
+          "   the K entry points; FP64 whatever the mixed-precision cutoff.  The",
+          "   derivative terms are the generator's gradient='a'/'c' terms",
+          "   (eri.py:85-152), which no reference generator emits.  No reference",
+          "   counterpart. */"]
+    for cls in k_classes():
+        L.append(f"int vlxb_computeExchangeGradient{cls.upper()}(" + ", ".join(kg_params(cls)) + ");")
+    L.append("")
     L.append("/* ---- Exchange: replace computeExchangeFock<ABCD> of gen_exchange.py:75-115 ---- */")
     for cls in k_classes():
         L.append(f"/* replaces computeExchangeFock{cls.upper()} (gen_exchange.py:75-115; "
@@ -310,6 +340,7 @@ def abi_cu():
         L.append(f"int coulomb_grad_{cls}(const CoulombArgs&, int64_t, cudaStream_t);")
     for cls in k_classes():
         L.append(f"int exchange_{cls}(const ExchangeArgs&, cudaStream_t);")
+        L.append(f"int exchange_grad_{cls}(const ExchangeArgs&, int64_t, cudaStream_t);")
     L += ["}  // namespace vlxb", "", 'extern "C" {', ""]
     for cls in j_classes():
         a, b, c, d = cls
@@ -371,6 +402,30 @@ def abi_cu():
         L.append("    A.omega = omega; A.thr = eri_threshold;")
         L.append(f"    return vlxb::exchange_{cls}(A, (cudaStream_t)stream);")
         L += ["}", ""]
+    for cls in k_classes():
+        a, b, c, d = cls
+        same = (c + d) == (a + b)
+        L.append(f"int vlxb_computeExchangeGradient{cls.upper()}(" + ", ".join(kg_params(cls)) + ")")
+        L.append("{")
+        L.append("    (void)boys_func_table; (void)boys_func_ft;")
+        L.append("    if (grad_stride > (uint64_t)INT64_MAX) return VLXB_EINVAL;")
+        L.append("    vlxb::ExchangeArgs A{};")
+        L.append(f"    A.mat_K = grad_K; A.pair_i = pair_inds_i_for_K_{a}{c}; A.pair_k = pair_inds_k_for_K_{a}{c};")
+        L.append(f"    A.n_ik = pair_inds_count_for_K_{a}{c};")
+        for x in ANG:
+            if x in cls:
+                L.append(f"    A.info[{LV[x]}] = {x}_prim_info; A.aoinds[{LV[x]}] = {x}_prim_aoinds; "
+                         f"A.count[{LV[x]}] = {x}_prim_count;")
+        L.append(f"    A.maxD = {b}{d}_max_D; A.D = mat_D_full_AO; A.naos = naos;")
+        cd = f"{a}{b}" if same else f"{c}{d}"
+        L.append(f"    A.Q_ab = Q_K_{a}{b}; A.Q_cd = Q_K_{cd};")
+        L.append(f"    A.Dinds_ab = D_inds_K_{a}{b}; A.Dinds_cd = D_inds_K_{cd};")
+        L.append(f"    A.displs_ab = pair_displs_K_{a}{b}; A.displs_cd = pair_displs_K_{cd};")
+        L.append(f"    A.counts_ab = pair_counts_K_{a}{b}; A.counts_cd = pair_counts_K_{cd};")
+        L.append(f"    A.pdata_ab = pair_data_K_{a}{b}; A.pdata_cd = pair_data_K_{cd};")
+        L.append("    A.omega = omega; A.thr = eri_threshold;")
+        L.append(f"    return vlxb::exchange_grad_{cls}(A, (int64_t)grad_stride, (cudaStream_t)stream);")
+        L += ["}", ""]
     # batched calls: runtime class -> the class units
     L += ["int vlxb_coulombBatch(int la, int lb, int lc, int ld, const VlxbBatchCall* c, void* stream)", "{",
           "    if (la < 0 || la > 2 || lb < 0 || lb > 2 || lc < 0 || lc > 2 || ld < 0 || ld > 2) return VLXB_EINVAL;",
@@ -430,6 +485,8 @@ def class_tu(cls, kind):
     else:
         L.append(f"int exchange_{cls}(const ExchangeArgs& a, cudaStream_t s) "
                  f"{{ return run_exchange<{la}, {lb}, {lc}, {ld}>(a, s); }}")
+        L.append(f"int exchange_grad_{cls}(const ExchangeArgs& a, int64_t gs, cudaStream_t s) "
+                 f"{{ return run_exchange_grad<{la}, {lb}, {lc}, {ld}>(a, gs, s); }}")
     L += ["}  // namespace vlxb", ""]
     return "\n".join(L)
 

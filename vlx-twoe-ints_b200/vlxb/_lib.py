@@ -66,6 +66,13 @@ class Lib:
             f.argtypes = [_ctype(p) for p in ps]
             f.restype = ctypes.c_int
             self.g_params[cls] = [ABI.pname(p) for p in ps]
+        self.kg_params = {}
+        for cls in ABI.k_classes():
+            ps = ABI.kg_params(cls)
+            f = getattr(self.cdll, f"vlxb_computeExchangeGradient{cls.upper()}")
+            f.argtypes = [_ctype(p) for p in ps]
+            f.restype = ctypes.c_int
+            self.kg_params[cls] = [ABI.pname(p) for p in ps]
         for cls in ABI.k_classes():
             ps = ABI.k_params(cls)
             f = getattr(self.cdll, f"vlxb_computeExchangeFock{cls.upper()}")
@@ -121,6 +128,11 @@ class Lib:
         vals = [args[n] for n in self.g_params[cls]]
         rc = getattr(self.cdll, f"vlxb_computeCoulombGradient{cls.upper()}")(*vals)
         self.check(rc, f"vlxb_computeCoulombGradient{cls.upper()}")
+
+    def exchange_grad(self, cls: str, args: dict) -> None:
+        vals = [args[n] for n in self.kg_params[cls]]
+        rc = getattr(self.cdll, f"vlxb_computeExchangeGradient{cls.upper()}")(*vals)
+        self.check(rc, f"vlxb_computeExchangeGradient{cls.upper()}")
 
     def exchange(self, cls: str, args: dict) -> None:
         vals = [args[n] for n in self.k_params[cls]]
