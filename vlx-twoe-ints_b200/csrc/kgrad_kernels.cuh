@@ -64,9 +64,11 @@ struct KGradShape {
     static constexpr int NY = (NC * NHK > NA * NHB) ? NC * NHK : NA * NHB;
     static constexpr int NT = (NA * NHK > NC * NHB) ? NA * NHK : NC * NHB;
     // lanes per quartet: a power of two near a quarter of the widest step
-    // (A-side contraction items), so that small classes run many quartets
-    // per warp (down to one per lane) and large ones a warp each
-    static constexpr int WIDE = NA * NHBP > NC * NHKP ? NA * NHBP : NC * NHKP;
+    // (the Y / T items and the Hermite indices of the R contractions), so that
+    // small classes run many quartets per warp (down to one per lane) and
+    // large ones a warp each
+    static constexpr int cmax(int x, int y) { return x > y ? x : y; }
+    static constexpr int WIDE = cmax(cmax(cmax(NC * NHK, NA * NHK), cmax(NA * NHB, NC * NHB)), cmax(NHBP, NHKP));
     static constexpr int SG = WIDE <= 4 ? 1 : WIDE <= 8 ? 2 : WIDE <= 16 ? 4 : WIDE <= 32 ? 8 : WIDE <= 64 ? 16 : 32;
     static constexpr int NG = 32 / SG;  // quartet groups per warp
     // doubles per group: R (two level buffers), R^{(n)}_{000}, E tables, D_bd, S_ab, S_cd, Y, T
@@ -93,12 +95,19 @@ exchange_grad_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity 
     __shared__ int16_t sIdx[NHKP][NHBP];  // index of R_{e+f}, -1 above level L + 1
     __shared__ uint32_t sTuv[NHL];
     __shared__ uint32_t sRec[NHL];  // R recurrence per entry (as coulomb_md_kernel)
+    __shared__ uint32_t sCart[4][10];  // exponents of component c of shell l: x | y << 4 | z << 8
     __shared__ double sDw[NA * NC];
     __shared__ double red[NW][6];
     __shared__ int s_pmin;
     __shared__ double sw[NW * NG][S::PER_GROUP];
     const KChunk ch{s_nl, s_n64, s_c64, s_c32};
 
+    for (int i = threadIdx.x; i < 40; i += NT_) {
+        const int l = i / 10, c = i % 10;
+        sCart[l][c] = c < ncart(l) ? (uint32_t)cart_x(l, c) | ((uint32_t)cart_y(l, c) << 4) |
+                                         ((uint32_t)cart_z(l, c) << 8)
+                                   : 0u;
+    }
     for (int i = threadIdx.x; i < NHL; i += NT_) {
         int n = 0;
         while (nherm(n) <= i) n++;
@@ -250,16 +259,19 @@ exchange_grad_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity 
                 // ---- A side: derivatives on i's centre
 #pragma unroll 1
                 for (int b = 0; b < NB; b++) {
-                    const int bx = cart_x(LB, b), by = cart_y(LB, b), bz = cart_z(LB, b);
+                    const uint32_t bp_ = sCart[LB][b];
+                    const int bx = bp_ & 15u, by = (bp_ >> 4) & 15u, bz = bp_ >> 8;
                     if (valid) {
                         for (int it = sub; it < NC * NHK; it += SG) {
                             const int c = it / NHK, f = it % NHK;
                             const uint32_t tf = sTuv[f];
                             const int t = tf & 255, u = (tf >> 8) & 255, v = tf >> 16;
-                            const int cx = cart_x(LC, c), cy = cart_y(LC, c), cz = cart_z(LC, c);
+                            const uint32_t cp_ = sCart[LC][c];
+                            const int cx = cp_ & 15u, cy = (cp_ >> 4) & 15u, cz = cp_ >> 8;
                             double y = 0.0;
                             for (int d = 0; d < ND; d++) {
-                                const int dx = cart_x(LD, d), dy = cart_y(LD, d), dz = cart_z(LD, d);
+                                const uint32_t dp_ = sCart[LD][d];
+                                const int dx = dp_ & 15u, dy = (dp_ >> 4) & 15u, dz = dp_ >> 8;
                                 const double e = Ek[0 * S::EK + (cx * (LD + 1) + dx) * LSK + t] *
                                                  Ek[1 * S::EK + (cy * (LD + 1) + dy) * LSK + u] *
                                                  Ek[2 * S::EK + (cz * (LD + 1) + dz) * LSK + v];
@@ -279,30 +291,46 @@ exchange_grad_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity 
                     }
                     __syncwarp();
                     if (valid) {
-                        for (int it = sub; it < NA * NHBP; it += SG) {
-                            const int a = it / NHBP, e = it % NHBP;
+                        // lanes over bra Hermite indices e; each R_{e+f} serves all a
+                        for (int e = sub; e < NHBP; e += SG) {
                             const uint32_t te = sTuv[e];
                             const int t = te & 255, u = (te >> 8) & 255, v = te >> 16;
-                            const int ax = cart_x(LA, a), ay = cart_y(LA, a), az = cart_z(LA, a);
-                            // 1-D factors E^{i,j}_t at i = a_x, a_x + 1, a_x - 1 (0 when i < 0)
-                            const double x0 = Eb[0 * S::EB + (ax * (LB + 1) + bx) * LSB + t];
-                            const double y0 = Eb[1 * S::EB + (ay * (LB + 1) + by) * LSB + u];
-                            const double z0 = Eb[2 * S::EB + (az * (LB + 1) + bz) * LSB + v];
-                            const double xp = Eb[0 * S::EB + ((ax + 1) * (LB + 1) + bx) * LSB + t];
-                            const double yp = Eb[1 * S::EB + ((ay + 1) * (LB + 1) + by) * LSB + u];
-                            const double zp = Eb[2 * S::EB + ((az + 1) * (LB + 1) + bz) * LSB + v];
-                            const double xm = ax > 0 ? Eb[0 * S::EB + ((ax - 1) * (LB + 1) + bx) * LSB + t] : 0.0;
-                            const double ym = ay > 0 ? Eb[1 * S::EB + ((ay - 1) * (LB + 1) + by) * LSB + u] : 0.0;
-                            const double zm = az > 0 ? Eb[2 * S::EB + ((az - 1) * (LB + 1) + bz) * LSB + v] : 0.0;
-                            const double dX = (al2 * xp - ax * xm) * y0 * z0;
-                            const double dY = x0 * (al2 * yp - ay * ym) * z0;
-                            const double dZ = x0 * y0 * (al2 * zp - az * zm);
-                            if (dX == 0.0 && dY == 0.0 && dZ == 0.0) continue;
-                            double s = 0.0;
-                            for (int f = 0; f < NHK; f++) s = fma(R[sIdx[f][e]], T[a * NHK + f], s);
-                            g[0] = fma(dX, s, g[0]);
-                            g[1] = fma(dY, s, g[1]);
-                            g[2] = fma(dZ, s, g[2]);
+                            double dE[NA][3];
+                            bool any = false;
+#pragma unroll
+                            for (int a = 0; a < NA; a++) {
+                                const uint32_t ap_ = sCart[LA][a];
+                                const int ax = ap_ & 15u, ay = (ap_ >> 4) & 15u, az = ap_ >> 8;
+                                // 1-D factors E^{i,j}_t at i = a_x, a_x + 1, a_x - 1 (0 when i < 0)
+                                const double x0 = Eb[0 * S::EB + (ax * (LB + 1) + bx) * LSB + t];
+                                const double y0 = Eb[1 * S::EB + (ay * (LB + 1) + by) * LSB + u];
+                                const double z0 = Eb[2 * S::EB + (az * (LB + 1) + bz) * LSB + v];
+                                const double xp = Eb[0 * S::EB + ((ax + 1) * (LB + 1) + bx) * LSB + t];
+                                const double yp = Eb[1 * S::EB + ((ay + 1) * (LB + 1) + by) * LSB + u];
+                                const double zp = Eb[2 * S::EB + ((az + 1) * (LB + 1) + bz) * LSB + v];
+                                const double xm = ax > 0 ? Eb[0 * S::EB + ((ax - 1) * (LB + 1) + bx) * LSB + t] : 0.0;
+                                const double ym = ay > 0 ? Eb[1 * S::EB + ((ay - 1) * (LB + 1) + by) * LSB + u] : 0.0;
+                                const double zm = az > 0 ? Eb[2 * S::EB + ((az - 1) * (LB + 1) + bz) * LSB + v] : 0.0;
+                                dE[a][0] = (al2 * xp - ax * xm) * y0 * z0;
+                                dE[a][1] = x0 * (al2 * yp - ay * ym) * z0;
+                                dE[a][2] = x0 * y0 * (al2 * zp - az * zm);
+                                any = any || dE[a][0] != 0.0 || dE[a][1] != 0.0 || dE[a][2] != 0.0;
+                            }
+                            if (!any) continue;
+                            double acc[NA];
+#pragma unroll
+                            for (int a = 0; a < NA; a++) acc[a] = 0.0;
+                            for (int f = 0; f < NHK; f++) {
+                                const double r = R[sIdx[f][e]];
+#pragma unroll
+                                for (int a = 0; a < NA; a++) acc[a] = fma(r, T[a * NHK + f], acc[a]);
+                            }
+#pragma unroll
+                            for (int a = 0; a < NA; a++) {
+                                g[0] = fma(dE[a][0], acc[a], g[0]);
+                                g[1] = fma(dE[a][1], acc[a], g[1]);
+                                g[2] = fma(dE[a][2], acc[a], g[2]);
+                            }
                         }
                     }
                     __syncwarp();
@@ -311,16 +339,19 @@ exchange_grad_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity 
                 // ---- C side: derivatives on k's centre
 #pragma unroll 1
                 for (int d = 0; d < ND; d++) {
-                    const int dx = cart_x(LD, d), dy = cart_y(LD, d), dz = cart_z(LD, d);
+                    const uint32_t dp_ = sCart[LD][d];
+                    const int dx = dp_ & 15u, dy = (dp_ >> 4) & 15u, dz = dp_ >> 8;
                     if (valid) {
                         for (int it = sub; it < NA * NHB; it += SG) {
                             const int a = it / NHB, e = it % NHB;
                             const uint32_t te = sTuv[e];
                             const int t = te & 255, u = (te >> 8) & 255, v = te >> 16;
-                            const int ax = cart_x(LA, a), ay = cart_y(LA, a), az = cart_z(LA, a);
+                            const uint32_t ap_ = sCart[LA][a];
+                            const int ax = ap_ & 15u, ay = (ap_ >> 4) & 15u, az = ap_ >> 8;
                             double y = 0.0;
                             for (int b = 0; b < NB; b++) {
-                                const int bx = cart_x(LB, b), by = cart_y(LB, b), bz = cart_z(LB, b);
+                                const uint32_t bp_ = sCart[LB][b];
+                                const int bx = bp_ & 15u, by = (bp_ >> 4) & 15u, bz = bp_ >> 8;
                                 const double e1 = Eb[0 * S::EB + (ax * (LB + 1) + bx) * LSB + t] *
                                                   Eb[1 * S::EB + (ay * (LB + 1) + by) * LSB + u] *
                                                   Eb[2 * S::EB + (az * (LB + 1) + bz) * LSB + v];
@@ -340,30 +371,46 @@ exchange_grad_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity 
                     }
                     __syncwarp();
                     if (valid) {
-                        for (int it = sub; it < NC * NHKP; it += SG) {
-                            const int c = it / NHKP, f = it % NHKP;
+                        // lanes over ket Hermite indices f; each R_{e+f} serves all c
+                        for (int f = sub; f < NHKP; f += SG) {
                             const uint32_t tf = sTuv[f];
                             const int t = tf & 255, u = (tf >> 8) & 255, v = tf >> 16;
-                            const int cx = cart_x(LC, c), cy = cart_y(LC, c), cz = cart_z(LC, c);
-                            const double x0 = Ek[0 * S::EK + (cx * (LD + 1) + dx) * LSK + t];
-                            const double y0 = Ek[1 * S::EK + (cy * (LD + 1) + dy) * LSK + u];
-                            const double z0 = Ek[2 * S::EK + (cz * (LD + 1) + dz) * LSK + v];
-                            const double xp = Ek[0 * S::EK + ((cx + 1) * (LD + 1) + dx) * LSK + t];
-                            const double yp = Ek[1 * S::EK + ((cy + 1) * (LD + 1) + dy) * LSK + u];
-                            const double zp = Ek[2 * S::EK + ((cz + 1) * (LD + 1) + dz) * LSK + v];
-                            const double xm = cx > 0 ? Ek[0 * S::EK + ((cx - 1) * (LD + 1) + dx) * LSK + t] : 0.0;
-                            const double ym = cy > 0 ? Ek[1 * S::EK + ((cy - 1) * (LD + 1) + dy) * LSK + u] : 0.0;
-                            const double zm = cz > 0 ? Ek[2 * S::EK + ((cz - 1) * (LD + 1) + dz) * LSK + v] : 0.0;
                             const double sg = ((t + u + v) & 1) ? -1.0 : 1.0;
-                            const double dX = sg * (ga2 * xp - cx * xm) * y0 * z0;
-                            const double dY = sg * x0 * (ga2 * yp - cy * ym) * z0;
-                            const double dZ = sg * x0 * y0 * (ga2 * zp - cz * zm);
-                            if (dX == 0.0 && dY == 0.0 && dZ == 0.0) continue;
-                            double s = 0.0;
-                            for (int e = 0; e < NHB; e++) s = fma(R[sIdx[f][e]], T[c * NHB + e], s);
-                            g[3] = fma(dX, s, g[3]);
-                            g[4] = fma(dY, s, g[4]);
-                            g[5] = fma(dZ, s, g[5]);
+                            double dE[NC][3];
+                            bool any = false;
+#pragma unroll
+                            for (int c = 0; c < NC; c++) {
+                                const uint32_t cp_ = sCart[LC][c];
+                                const int cx = cp_ & 15u, cy = (cp_ >> 4) & 15u, cz = cp_ >> 8;
+                                const double x0 = Ek[0 * S::EK + (cx * (LD + 1) + dx) * LSK + t];
+                                const double y0 = Ek[1 * S::EK + (cy * (LD + 1) + dy) * LSK + u];
+                                const double z0 = Ek[2 * S::EK + (cz * (LD + 1) + dz) * LSK + v];
+                                const double xp = Ek[0 * S::EK + ((cx + 1) * (LD + 1) + dx) * LSK + t];
+                                const double yp = Ek[1 * S::EK + ((cy + 1) * (LD + 1) + dy) * LSK + u];
+                                const double zp = Ek[2 * S::EK + ((cz + 1) * (LD + 1) + dz) * LSK + v];
+                                const double xm = cx > 0 ? Ek[0 * S::EK + ((cx - 1) * (LD + 1) + dx) * LSK + t] : 0.0;
+                                const double ym = cy > 0 ? Ek[1 * S::EK + ((cy - 1) * (LD + 1) + dy) * LSK + u] : 0.0;
+                                const double zm = cz > 0 ? Ek[2 * S::EK + ((cz - 1) * (LD + 1) + dz) * LSK + v] : 0.0;
+                                dE[c][0] = sg * (ga2 * xp - cx * xm) * y0 * z0;
+                                dE[c][1] = sg * x0 * (ga2 * yp - cy * ym) * z0;
+                                dE[c][2] = sg * x0 * y0 * (ga2 * zp - cz * zm);
+                                any = any || dE[c][0] != 0.0 || dE[c][1] != 0.0 || dE[c][2] != 0.0;
+                            }
+                            if (!any) continue;
+                            double acc[NC];
+#pragma unroll
+                            for (int c = 0; c < NC; c++) acc[c] = 0.0;
+                            for (int e = 0; e < NHB; e++) {
+                                const double r = R[sIdx[f][e]];
+#pragma unroll
+                                for (int c = 0; c < NC; c++) acc[c] = fma(r, T[c * NHB + e], acc[c]);
+                            }
+#pragma unroll
+                            for (int c = 0; c < NC; c++) {
+                                g[3] = fma(dE[c][0], acc[c], g[3]);
+                                g[4] = fma(dE[c][1], acc[c], g[4]);
+                                g[5] = fma(dE[c][2], acc[c], g[5]);
+                            }
                         }
                     }
                     __syncwarp();
