@@ -150,3 +150,43 @@ def test_device_lists_exchange_gradient(system, kref):
     g_or, _ = kref
     g = gradient.exchange_gradient(wl.mol, wl.D, wl.threshold).cpu().numpy()
     assert np.abs(g - g_or).max() <= 1e-10 * max(1.0, np.abs(g_or).max())
+
+
+def test_exchange_gradient_argument_checks_and_edges(system):
+    """Stride below the (i, k) count: VLXB_EINVAL, nothing written.  A
+    threshold that screens every quartet: exact zeros.  An empty (i, k) list:
+    success, nothing written."""
+    wl, rl, _, _ = system
+    dl = fock.to_device(rl)
+    s = torch.cuda.current_stream().cuda_stream
+    L = lib()
+    n = len(rl.kpairs["pp"].pair_i)  # class (pd|pd): (i, k) list of type pp
+    G = torch.zeros((6, n), dtype=torch.float64, device="cuda")
+    args = gradient.kgrad_args(dl, "pdpd", G, 0, n - 1, s)
+    rc = getattr(L.cdll, "vlxb_computeExchangeGradientPDPD")(*[args[p] for p in L.kg_params["pdpd"]])
+    assert rc == 1  # VLXB_EINVAL
+    dl.threshold = 1e30
+    nj = len(rl.jlists["pd"].first)
+    GJ = torch.zeros((6, nj), dtype=torch.float64, device="cuda")
+    L.exchange_grad("pdpd", gradient.kgrad_args(dl, "pdpd", G, 0, n, s))
+    L.coulomb_grad("pdpd", gradient.grad_args(dl, "pdpd", GJ, 0, nj, s))
+    torch.cuda.synchronize()
+    assert float(G.abs().max()) == 0.0 and float(GJ.abs().max()) == 0.0
+    dl.threshold = wl.threshold
+    args = gradient.kgrad_args(dl, "pdpd", G, 0, n, s)
+    args["pair_inds_count_for_K_pp"] = 0
+    L.exchange_grad("pdpd", args)
+    torch.cuda.synchronize()
+    assert float(G.abs().max()) == 0.0
+
+
+def test_gradient_fold_of_zero_entries():
+    """A system whose lists are all empty after screening folds to zeros."""
+    lib().init(0)
+    wl = basis.config_custom(2, 3.0, {0: 1, 1: 1}, 1, 0.3, 2.5, 1, 1e-12, 5)
+    rl = lists.build_lists(wl.mol, wl.D, 1e30, fock.gpu_schwarz_fn())
+    dl = fock.to_device(rl)
+    gj = gradient.CoulombGradient(dl, wl.mol).compute().cpu().numpy()
+    gk = gradient.ExchangeGradient(dl, wl.mol).compute().cpu().numpy()
+    assert gj.shape == (2, 3) and gk.shape == (2, 3)
+    assert not gj.any() and not gk.any()

@@ -168,7 +168,8 @@ def to_atoms(G: torch.Tensor, gmap: GradientMap, weight: torch.Tensor | None = N
     if out is None:
         out = torch.empty((gmap.natoms, 3), dtype=torch.float64, device=gmap.device)
     wp = weight.data_ptr() if weight is not None and weight.numel() else 0
-    lib().check(lib().cdll.vlxb_pairGradientToAtoms(G.data_ptr(), G.shape[1], wp, gmap.rowptr.data_ptr(),
+    stride = G.shape[1] if gmap.total else 0  # no entries: nothing is read
+    lib().check(lib().cdll.vlxb_pairGradientToAtoms(G.data_ptr(), stride, wp, gmap.rowptr.data_ptr(),
                                                     gmap.src.data_ptr() if gmap.src.numel() else 0,
                                                     gmap.natoms, out.data_ptr(), st.cuda_stream),
                 "vlxb_pairGradientToAtoms")
