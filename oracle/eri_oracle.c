@@ -249,6 +249,43 @@ void oracle_eri_shell_quartet(int la, int lb, int lc, int ld,
     ctx_free(c);
 }
 
+/* Derivatives of the bare integrals of one primitive shell quartet with
+   respect to one centre (center 0..3 = A, B, C, D), by the Obara-Saika
+   derivative relation (eri.py:85-175, the generator's gradient='a'..'d'):
+   d/dX_g (.. x ..) = 2 zeta_x (.. x+1_g ..) - x_g (.. x-1_g ..).
+   out[(g * na * nb + ...)] = out[g][ca][cb][cc][cd], g = 0..2. */
+void oracle_eri_shell_quartet_grad(int la, int lb, int lc, int ld, int center,
+                                   double ai, const double* A, double aj, const double* B,
+                                   double ak, const double* C, double al, const double* D,
+                                   double omega, double* out)
+{
+    OrCtx* c = ctx_new_nb(OR_MAXL + 2);
+    int L = la + lb + lc + ld + 1;
+    setup_quartet(c, L, ai, A, aj, B, ak, C, al, D, omega);
+    int na = ncart_of[la], nb = ncart_of[lb], nc = ncart_of[lc], nd = ncart_of[ld];
+    const double zeta[4] = {ai, aj, ak, al};
+    size_t ncomp = (size_t)na * nb * nc * nd;
+    for (int g = 0; g < 3; g++)
+    for (int ia = 0; ia < na; ia++)
+    for (int ib = 0; ib < nb; ib++)
+    for (int ic = 0; ic < nc; ic++)
+    for (int id = 0; id < nd; id++) {
+        int v[4][3];
+        const int* src[4] = {cart_comp(la, ia), cart_comp(lb, ib), cart_comp(lc, ic), cart_comp(ld, id)};
+        for (int t = 0; t < 4; t++)
+            for (int x = 0; x < 3; x++) v[t][x] = src[t][x];
+        int n = v[center][g];
+        v[center][g] += 1;
+        double val = 2.0 * zeta[center] * quartet_component(c, v[0], v[1], v[2], v[3]);
+        if (n > 0) {
+            v[center][g] -= 2;
+            val -= n * quartet_component(c, v[0], v[1], v[2], v[3]);
+        }
+        out[(size_t)g * ncomp + ((ia * nb + ib) * nc + ic) * nd + id] = val;
+    }
+    ctx_free(c);
+}
+
 /* prim_info layout of gen_coulomb.py:170-180: row 0 exponent, rows 2..4 xyz,
    row stride = prim_count; prim-cart index i -> primitive i / ncart,
    component i % ncart. */

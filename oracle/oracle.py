@@ -41,6 +41,11 @@ def lib():
             + [ctypes.c_double, _f64p] * 4
             + [ctypes.c_double, _f64p]
         )
+        L.oracle_eri_shell_quartet_grad.argtypes = (
+            [ctypes.c_int] * 5
+            + [ctypes.c_double, _f64p] * 4
+            + [ctypes.c_double, _f64p]
+        )
         L.oracle_coulomb_fock.argtypes = (
             [ctypes.c_int] * 4
             + [_f64p, ctypes.POINTER(_f64p), _u32p, _f64p, _f64p, _f64p,
@@ -121,6 +126,22 @@ def eri_shell_quartet(la, lb, lc, ld, ai, A, aj, B, ak, C, al, D, omega=0.0):
     lib().oracle_eri_shell_quartet(la, lb, lc, ld, *args, ctypes.c_double(omega),
                                    out.ctypes.data_as(_f64p))
     return out.reshape(nc[la], nc[lb], nc[lc], nc[ld])
+
+
+def eri_shell_quartet_grad(la, lb, lc, ld, center, ai, A, aj, B, ak, C, al, D, omega=0.0):
+    """d/dX_g of the bare integrals, X the centre `center` (0..3 = A..D):
+    array (3, na, nb, nc, nd)."""
+    nc = [1, 3, 6]
+    out = np.zeros(3 * nc[la] * nc[lb] * nc[lc] * nc[ld])
+    args = []
+    keep = []
+    for al_, R in ((ai, A), (aj, B), (ak, C), (al, D)):
+        r, p = _f(R)
+        keep.append(r)
+        args += [ctypes.c_double(al_), p]
+    lib().oracle_eri_shell_quartet_grad(la, lb, lc, ld, int(center), *args, ctypes.c_double(omega),
+                                        out.ctypes.data_as(_f64p))
+    return out.reshape(3, nc[la], nc[lb], nc[lc], nc[ld])
 
 
 def _prim_tables(prim_info, prim_count, prim_aoinds=None):

@@ -18,6 +18,11 @@ Writes:
   jk_tiny.npz         a two-atom s/p/d system: the ABI arrays of every J class
                       (36) and K class (54) and mat_J / mat_K computed with the
                       emitted kernels' loop semantics (break on sorted lists).
+  eri_grad_components.npz  every s/p/d class, the generator's derivative
+                      expressions (write_eri_code(..., gradient='a'..'d'),
+                      eriwriter.py:72-86, eri.py:85-175) for one centre per
+                      class (rotating a..d; omega 0 / 0.4), all components and
+                      directions.
 """
 from __future__ import annotations
 
@@ -62,6 +67,18 @@ class Classes:
             src = self._w(cls, indent=0)
             self._cache[cls] = compile("(" + src + ")", f"<eri {cls}>", "eval")
         return self._cache[cls]
+
+    def code_grad(self, cls, centre):
+        """Compiled derivative expression of write_eri_code(cls, gradient=centre)
+        (eriwriter.py:72-86) and the order of its Boys array (F<m>_t)."""
+        key = (cls, centre)
+        if key not in self._cache:
+            import re
+
+            src = self._w(cls, indent=0, gradient=centre)
+            m = int(re.search(r"F(\d+)_t", src).group(1))
+            self._cache[key] = (compile("(" + src + ")", f"<eri {cls} d{centre}>", "eval"), m)
+        return self._cache[key]
 
 
 def comp_indices(x, comp):
@@ -123,6 +140,84 @@ def eval_component(classes, cls, ai, ri, aj, rj, ak, rk, al, rl, comps, omega, F
         ns[f"d{n}"] = v
         ns[f"QD_{n}"] = (-ak * inv_S2) * (rl[v] - rk[v])
     return lam * eval(classes.code(cls), {}, ns)
+
+
+def eval_grad_component(classes, cls, centre, g, ai, ri, aj, rj, ak, rk, al, rl, comps, omega):
+    """Lambda * the reference's derivative expression d/dX_g of one component
+    quartet, X the centre `centre` ('a'..'d').  Binds the names of
+    eval_component plus a_i..a_l (the four exponents), g / grad_cart_ind (the
+    Cartesian direction) and PA_x, PB_x, QC_x, QD_x (the g components of
+    P - A, P - B, Q - C, Q - D), as the generator's replacements at
+    eriwriter.py:152-156 name them."""
+    code, M = classes.code_grad(cls, centre)
+    S1 = ai + aj
+    inv_S1 = 1.0 / S1
+    S2 = ak + al
+    inv_S2 = 1.0 / S2
+    inv_S4 = 1.0 / (S1 + S2)
+    PQ = [(ak * rk[x] + al * rl[x]) * inv_S2 - (ai * ri[x] + aj * rj[x]) * inv_S1 for x in range(3)]
+    r2 = PQ[0] ** 2 + PQ[1] ** 2 + PQ[2] ** 2
+    rho = S1 * S2 * inv_S4
+    d2 = 1.0
+    if omega != 0.0:
+        d2 = omega * omega / (rho + omega * omega)
+    lam = math.sqrt(4.0 * rho * d2 / math.pi)
+    F = boys_mp(M, rho * d2 * r2)
+    if omega != 0.0:
+        F = [F[m] * d2 ** m for m in range(M + 1)]
+    ns = {"PQ": PQ, "S1": S1, "S2": S2, "inv_S1": inv_S1, "inv_S2": inv_S2, "inv_S4": inv_S4,
+          "delta": [[1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]], f"F{M}_t": F,
+          "a_i": ai, "a_j": aj, "a_k": ak, "a_l": al, "g": g, "grad_cart_ind": g,
+          "PA_x": (aj * inv_S1) * (rj[g] - ri[g]), "PB_x": (-ai * inv_S1) * (rj[g] - ri[g]),
+          "QC_x": (al * inv_S2) * (rl[g] - rk[g]), "QD_x": (-ak * inv_S2) * (rl[g] - rk[g])}
+    a, b, c, d = cls
+    ia, jb, kc, ld = comps
+    for n, v in enumerate(comp_indices(a, ia)):
+        ns[f"a{n}"] = v
+        ns[f"PA_{n}"] = (aj * inv_S1) * (rj[v] - ri[v])
+    for n, v in enumerate(comp_indices(b, jb)):
+        ns[f"b{n}"] = v
+        ns[f"PB_{n}"] = (-ai * inv_S1) * (rj[v] - ri[v])
+    for n, v in enumerate(comp_indices(c, kc)):
+        ns[f"c{n}"] = v
+        ns[f"QC_{n}"] = (al * inv_S2) * (rl[v] - rk[v])
+    for n, v in enumerate(comp_indices(d, ld)):
+        ns[f"d{n}"] = v
+        ns[f"QD_{n}"] = (-ak * inv_S2) * (rl[v] - rk[v])
+    return lam * eval(code, {}, ns)
+
+
+def make_grad_components(classes, rng):
+    """Every s/p/d class once, the differentiated centre rotating over
+    a, b, c, d and omega over 0 / 0.4 with the class index; all components,
+    all three directions."""
+    out = {}
+    t = 0
+    for a in "spd":
+        for b in "spd":
+            for c in "spd":
+                for d in "spd":
+                    cls = a + b + c + d
+                    centre = "abcd"[t % 4]
+                    omega = 0.4 if (t // 4) % 2 else 0.0
+                    t += 1
+                    ex = rng.uniform(0.3, 2.5, size=4)
+                    R = rng.uniform(-1.2, 1.2, size=(4, 3))
+                    vals = np.zeros((3, NCART[a], NCART[b], NCART[c], NCART[d]))
+                    for g in range(3):
+                        for ia in range(NCART[a]):
+                            for ib in range(NCART[b]):
+                                for ic in range(NCART[c]):
+                                    for id_ in range(NCART[d]):
+                                        vals[g, ia, ib, ic, id_] = eval_grad_component(
+                                            classes, cls, centre, g, ex[0], R[0], ex[1], R[1], ex[2], R[2],
+                                            ex[3], R[3], (ia, ib, ic, id_), omega)
+                    out[f"{cls}_centre"] = np.array(["abcd".index(centre)])
+                    out[f"{cls}_exps"] = ex
+                    out[f"{cls}_centers"] = R
+                    out[f"{cls}_omega"] = np.array([omega])
+                    out[f"{cls}_vals"] = vals
+    return out
 
 
 # ------------------------------------------------------------ component set
@@ -359,13 +454,17 @@ def build_tiny(classes, rng):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", choices=["components", "tiny"], default=None)
+    ap.add_argument("--only", choices=["components", "tiny", "grad"], default=None)
     args = ap.parse_args()
     classes = Classes(args.ref)
     if args.only in (None, "components"):
         comp = make_components(classes, np.random.default_rng(1234))
         np.savez_compressed(os.path.join(HERE, "eri_components.npz"), **comp)
         print("eri_components.npz:", len(comp), "arrays")
+    if args.only in (None, "grad"):
+        grad = make_grad_components(classes, np.random.default_rng(2468))
+        np.savez_compressed(os.path.join(HERE, "eri_grad_components.npz"), **grad)
+        print("eri_grad_components.npz:", len(grad), "arrays")
     if args.only in (None, "tiny"):
         tiny = build_tiny(classes, np.random.default_rng(4321))
         np.savez_compressed(os.path.join(HERE, "jk_tiny.npz"), **tiny)

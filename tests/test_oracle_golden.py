@@ -5,6 +5,8 @@ expressions (eriwriter.py:35-160) evaluated for all 81 s/p/d classes, with and
 without range separation.  jk_tiny.npz: mat_J / mat_K of every J (36) and K (54)
 class of a two-atom s/p/d system, computed with the emitted kernels' loop
 semantics (gen_coulomb.py:205-297, gen_exchange.py:139-342).
+eri_grad_components.npz: the generator's derivative expressions
+(gradient='a'..'d', eriwriter.py:72-86) for every s/p/d class.
 """
 import numpy as np
 import pytest
@@ -40,6 +42,33 @@ def test_components_all_classes():
                         g = z[f"{cls}_{tag}_vals"]
                         err = np.abs(v - g).max() / np.abs(g).max()
                         worst = max(worst, err)
+    assert worst < 1e-12, worst
+
+
+def test_gradient_components_all_classes():
+    """The oracle's derivative integrals (Obara-Saika derivative relation)
+    against the reference generator's own derivative expressions
+    (write_eri_code(..., gradient='a'..'d'), eri_grad_components.npz): every
+    s/p/d class, one centre each (rotating over a..d), omega 0 and 0.4."""
+    z = np.load(f"{tf.HERE}/golden/eri_grad_components.npz")
+    worst = 0.0
+    seen = set()
+    for a in "spd":
+        for b in "spd":
+            for c in "spd":
+                for d in "spd":
+                    cls = a + b + c + d
+                    ex = z[f"{cls}_exps"]
+                    R = z[f"{cls}_centers"]
+                    w = float(z[f"{cls}_omega"][0])
+                    centre = int(z[f"{cls}_centre"][0])
+                    seen.add((centre, w))
+                    v = oracle.eri_shell_quartet_grad(LV[a], LV[b], LV[c], LV[d], centre, ex[0], R[0], ex[1], R[1],
+                                                      ex[2], R[2], ex[3], R[3], w)
+                    g = z[f"{cls}_vals"]
+                    err = np.abs(v - g).max() / np.abs(g).max()
+                    worst = max(worst, err)
+    assert len(seen) == 8  # every centre with both omegas
     assert worst < 1e-12, worst
 
 
