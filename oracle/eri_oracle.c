@@ -218,25 +218,33 @@ static void ctx_free(OrCtx* c) { free(c->memo); free(c->stamp); free(c); }
 static const int cart_s[1][3] = {{0, 0, 0}};
 static const int cart_p[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
 static const int cart_d[6][3] = {{2, 0, 0}, {1, 1, 0}, {1, 0, 1}, {0, 2, 0}, {0, 1, 1}, {0, 0, 2}};
-static const int ncart_of[3] = {1, 3, 6};
+/* f in the same convention (x^3 first, then by decreasing y power): the
+   component tables the reference's emitted kernels would use for a third
+   index (sorted index triples xxx, xxy, ..., zzz). */
+static const int cart_f[10][3] = {{3, 0, 0}, {2, 1, 0}, {2, 0, 1}, {1, 2, 0}, {1, 1, 1},
+                                  {1, 0, 2}, {0, 3, 0}, {0, 2, 1}, {0, 1, 2}, {0, 0, 3}};
+static const int ncart_of[4] = {1, 3, 6, 10};
 
 static const int* cart_comp(int l, int k)
 {
     if (l == 0) return cart_s[0];
     if (l == 1) return cart_p[k];
-    return cart_d[k];
+    if (l == 2) return cart_d[k];
+    return cart_f[k];
 }
 
 /* ------------------------------------------------------- public helpers */
 
 /* Bare integrals (ab|cd)/(S_ab S_cd) for every Cartesian component quartet of
-   one primitive shell quartet; out[((ca*nb+cb)*nc+cc)*nd+cd]. */
+   one primitive shell quartet; out[((ca*nb+cb)*nc+cc)*nd+cd].  Shells up to
+   f (l <= 3). */
 void oracle_eri_shell_quartet(int la, int lb, int lc, int ld,
                               double ai, const double* A, double aj, const double* B,
                               double ak, const double* C, double al, const double* D,
                               double omega, double* out)
 {
-    OrCtx* c = ctx_new();
+    int emax = (la + lb > lc + ld) ? la + lb : lc + ld;
+    OrCtx* c = ctx_new_nb(emax + 1 > OR_MAXL + 1 ? emax + 1 : OR_MAXL + 1);
     int L = la + lb + lc + ld;
     setup_quartet(c, L, ai, A, aj, B, ak, C, al, D, omega);
     int na = ncart_of[la], nb = ncart_of[lb], nc = ncart_of[lc], nd = ncart_of[ld];

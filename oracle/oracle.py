@@ -114,8 +114,9 @@ def boys_mpmath(M: int, T: float, dps: int = 40) -> list:
 
 
 def eri_shell_quartet(la, lb, lc, ld, ai, A, aj, B, ak, C, al, D, omega=0.0):
-    """Bare (ab|cd)/(S_ab S_cd) for all Cartesian components, shape (na,nb,nc,nd)."""
-    nc = [1, 3, 6]
+    """Bare (ab|cd)/(S_ab S_cd) for all Cartesian components, shape (na,nb,nc,nd);
+    shells up to f."""
+    nc = [1, 3, 6, 10]
     out = np.zeros(nc[la] * nc[lb] * nc[lc] * nc[ld])
     args = []
     keep = []

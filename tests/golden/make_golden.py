@@ -23,6 +23,9 @@ Writes:
                       eriwriter.py:72-86, eri.py:85-175) for one centre per
                       class (rotating a..d; omega 0 / 0.4), all components and
                       directions.
+  eri_f_components.npz  twelve classes with f centres (one or two), all
+                      components, from the reference's symbolic engine with
+                      three Cartesian indices on the f centres (eri.py).
 """
 from __future__ import annotations
 
@@ -34,9 +37,12 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-NCART = {"s": 1, "p": 3, "d": 6}
-LVAL = {"s": 0, "p": 1, "d": 2}
+NCART = {"s": 1, "p": 3, "d": 6, "f": 10}
+LVAL = {"s": 0, "p": 1, "d": 2, "f": 3}
 D_CART = [(0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2)]  # gen_coulomb.py:143-148
+# f components in the same convention (sorted index triples: xxx, xxy, xxz, xyy,
+# xyz, xzz, yyy, yyz, yzz, zzz)
+F_CART = [(i, j, k) for i in range(3) for j in range(i, 3) for k in range(j, 3)]
 
 
 def boys_mp(M, T):
@@ -64,9 +70,34 @@ class Classes:
 
     def code(self, cls):
         if cls not in self._cache:
-            src = self._w(cls, indent=0)
+            src = self._w_f(cls) if "f" in cls else self._w(cls, indent=0)
             self._cache[cls] = compile("(" + src + ")", f"<eri {cls}>", "eval")
         return self._cache[cls]
+
+    def _w_f(self, cls):
+        """write_eri_code for a class with f centres.  The writer maps only the
+        letters p and d to index lists (eriwriter.py:44-62) while its ERI
+        class takes any number of Cartesian indices per centre (eri.py:59
+        labels up to I), so the ERI constructor it calls is wrapped to give
+        the f centres three indices (x0, x1, x2); everything else is the
+        reference's own pipeline."""
+        import eriwriter
+
+        orig = eriwriter.ERI
+        fpos = [n for n, x in enumerate(cls) if x == "f"]
+
+        class ERIWithF(orig):
+            def __init__(self, la, lb, lc, ld, *rest):
+                lists = [list(la), list(lb), list(lc), list(ld)]
+                for n in fpos:
+                    lists[n] = [f"{'abcd'[n]}{k}" for k in range(3)]
+                super().__init__(*lists, *rest)
+
+        eriwriter.ERI = ERIWithF
+        try:
+            return self._w(cls.replace("f", "s"), indent=0)
+        finally:
+            eriwriter.ERI = orig
 
     def code_grad(self, cls, centre):
         """Compiled derivative expression of write_eri_code(cls, gradient=centre)
@@ -87,6 +118,8 @@ def comp_indices(x, comp):
         return [comp % 3]
     if x == "d":
         return list(D_CART[comp % 6])
+    if x == "f":
+        return list(F_CART[comp % 10])
     return []
 
 
@@ -217,6 +250,33 @@ def make_grad_components(classes, rng):
                     out[f"{cls}_centers"] = R
                     out[f"{cls}_omega"] = np.array([omega])
                     out[f"{cls}_vals"] = vals
+    return out
+
+
+F_CLASSES = ["fsss", "sfss", "ssfs", "sssf", "fpps", "psfp", "fdss", "sdsf", "ffss", "fsfs", "fpfp", "dfsd"]
+
+
+def make_f_components(classes, rng):
+    """Classes with f centres, from the reference's symbolic engine (see
+    Classes._w_f): all components, omega 0 and 0.4 alternating."""
+    out = {}
+    for t, cls in enumerate(F_CLASSES):
+        a, b, c, d = cls
+        omega = 0.4 if t % 2 else 0.0
+        ex = rng.uniform(0.3, 2.5, size=4)
+        R = rng.uniform(-1.2, 1.2, size=(4, 3))
+        vals = np.zeros((NCART[a], NCART[b], NCART[c], NCART[d]))
+        Fc = {}
+        for ia in range(NCART[a]):
+            for ib in range(NCART[b]):
+                for ic in range(NCART[c]):
+                    for id_ in range(NCART[d]):
+                        vals[ia, ib, ic, id_] = eval_component(classes, cls, ex[0], R[0], ex[1], R[1], ex[2], R[2],
+                                                               ex[3], R[3], (ia, ib, ic, id_), omega, Fc)
+        out[f"{cls}_exps"] = ex
+        out[f"{cls}_centers"] = R
+        out[f"{cls}_omega"] = np.array([omega])
+        out[f"{cls}_vals"] = vals
     return out
 
 
@@ -454,7 +514,7 @@ def build_tiny(classes, rng):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", choices=["components", "tiny", "grad"], default=None)
+    ap.add_argument("--only", choices=["components", "tiny", "grad", "f"], default=None)
     args = ap.parse_args()
     classes = Classes(args.ref)
     if args.only in (None, "components"):
@@ -465,6 +525,10 @@ def main():
         grad = make_grad_components(classes, np.random.default_rng(2468))
         np.savez_compressed(os.path.join(HERE, "eri_grad_components.npz"), **grad)
         print("eri_grad_components.npz:", len(grad), "arrays")
+    if args.only in (None, "f"):
+        fc = make_f_components(classes, np.random.default_rng(1357))
+        np.savez_compressed(os.path.join(HERE, "eri_f_components.npz"), **fc)
+        print("eri_f_components.npz:", len(fc), "arrays")
     if args.only in (None, "tiny"):
         tiny = build_tiny(classes, np.random.default_rng(4321))
         np.savez_compressed(os.path.join(HERE, "jk_tiny.npz"), **tiny)

@@ -7,6 +7,7 @@ class of a two-atom s/p/d system, computed with the emitted kernels' loop
 semantics (gen_coulomb.py:205-297, gen_exchange.py:139-342).
 eri_grad_components.npz: the generator's derivative expressions
 (gradient='a'..'d', eriwriter.py:72-86) for every s/p/d class.
+eri_f_components.npz: twelve classes with f centres from the same engine.
 """
 import numpy as np
 import pytest
@@ -14,7 +15,7 @@ import pytest
 from oracle import oracle
 import tiny_fixture as tf
 
-LV = {"s": 0, "p": 1, "d": 2}
+LV = {"s": 0, "p": 1, "d": 2, "f": 3}
 
 
 def test_boys_against_mpmath():
@@ -69,6 +70,22 @@ def test_gradient_components_all_classes():
                     err = np.abs(v - g).max() / np.abs(g).max()
                     worst = max(worst, err)
     assert len(seen) == 8  # every centre with both omegas
+    assert worst < 1e-12, worst
+
+
+def test_f_shell_components():
+    """Classes with f centres: the oracle against the reference's symbolic
+    engine run with three Cartesian indices on those centres
+    (eri_f_components.npz; one and two f centres, omega 0 and 0.4)."""
+    z = np.load(f"{tf.HERE}/golden/eri_f_components.npz")
+    classes = sorted({k.split("_")[0] for k in z.files})
+    assert len(classes) == 12
+    worst = 0.0
+    for cls in classes:
+        ex, R, w = z[f"{cls}_exps"], z[f"{cls}_centers"], float(z[f"{cls}_omega"][0])
+        v = oracle.eri_shell_quartet(*(LV[x] for x in cls), ex[0], R[0], ex[1], R[1], ex[2], R[2], ex[3], R[3], w)
+        g = z[f"{cls}_vals"]
+        worst = max(worst, np.abs(v - g).max() / np.abs(g).max())
     assert worst < 1e-12, worst
 
 
