@@ -5,6 +5,7 @@
 #include "engine.cuh"
 #include "jk_kernels.cuh"
 #include "md_kernels.cuh"
+#include "jgrad_kernels.cuh"
 #include "kgrad_kernels.cuh"
 
 namespace vlxb {
@@ -61,7 +62,7 @@ struct ExchangeArgs {
 
 // Coulomb class call on a given arena (pool, static or measuring) with given
 // Boys tables and quartet counter (may be null).  G = 1: the bra-centre
-// derivatives of J instead (coulomb_md_kernel<..., 1>), written to
+// derivatives of J instead (coulomb_grad_kernel), written to
 // a.mat_J[k * gstride + o], k = 0..5.
 template <int LA, int LB, int LC, int LD, int G = 0>
 int run_coulomb_impl(const CoulombArgs& a, cudaStream_t st, Arena& ar, const BoysTabs& tab,
@@ -107,12 +108,13 @@ int run_coulomb_impl(const CoulombArgs& a, cudaStream_t st, Arena& ar, const Boy
     if ((int64_t)grid > (int64_t)a.n_ab) grid = (int)a.n_ab;
     for (int pm = 0; pm < (cut > 0.0 ? 2 : 1); pm++) {
         if constexpr (G == 1) {
+            constexpr int GT = JGradShape<LA, LB, LC, LD>::THREADS;
             if (pm == 0)
-                coulomb_md_kernel<LA, LB, LC, LD, 0, 1><<<grid, MD_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab,
-                                                                                     nullptr, cut, gstride);
+                coulomb_grad_kernel<LA, LB, LC, LD, 0><<<grid, GT, 0, st>>>(bra, ket, a.mat_J, gstride, a.thr, tab,
+                                                                            cut);
             else
-                coulomb_md_kernel<LA, LB, LC, LD, 1, 1><<<grid, MD_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab,
-                                                                                     nullptr, cut, gstride);
+                coulomb_grad_kernel<LA, LB, LC, LD, 1><<<grid, GT, 0, st>>>(bra, ket, a.mat_J, gstride, a.thr, tab,
+                                                                            cut);
         } else if (jvar == 2) {
             if (pm == 0)
                 coulomb_md_kernel<LA, LB, LC, LD, 0><<<grid, MD_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc,

@@ -22,6 +22,9 @@
 //   dJ_ab/dA_x = S_ab sum_e (2 alpha E^{a+1x,b}_e - a_x E^{a-1x,b}_e) X_e,
 // the same with beta = p - alpha on B.  Output: mat_J[k * gstride + o],
 // k = 0..2 the A components, 3..5 the B components, accumulated with +=.
+// The library's gradient entry points use coulomb_grad_kernel
+// (jgrad_kernels.cuh), the same mathematics with several quartets per warp;
+// this one-quartet-per-warp form is not dispatched.
 #pragma once
 #include <type_traits>
 
