@@ -51,3 +51,25 @@ def test_python_binding_matches_header():
     for cls in ABI.k_classes():
         sig = f"int vlxb_computeExchangeFock{cls.upper()}(" + ", ".join(ABI.k_params(cls)) + ");"
         assert sig in hdr
+
+
+def test_gradient_entry_points_declared_and_bound():
+    """One Coulomb-gradient entry point per J class and one exchange-gradient
+    entry point per K class, with the argument lists the Python binding uses,
+    plus the per-atom fold."""
+    from vlxb._lib import ABI
+
+    names = declared()
+    jg = [n for n in names if n.startswith("vlxb_computeCoulombGradient")]
+    kg = [n for n in names if n.startswith("vlxb_computeExchangeGradient")]
+    assert len(jg) == 36 and len(kg) == 54
+    assert "vlxb_pairGradientToAtoms" in names
+    hdr = open(HDR).read()
+    for cls in ABI.j_classes():
+        ps = ABI.g_params(cls)
+        assert ps[:2] == ["double* grad_J", "uint64_t grad_stride"] and ps[2:] == ABI.j_params(cls)[1:]
+        assert f"int vlxb_computeCoulombGradient{cls.upper()}(" + ", ".join(ps) + ");" in hdr
+    for cls in ABI.k_classes():
+        ps = ABI.kg_params(cls)
+        assert ps[:2] == ["double* grad_K", "uint64_t grad_stride"] and ps[2:] == ABI.k_params(cls)[1:]
+        assert f"int vlxb_computeExchangeGradient{cls.upper()}(" + ", ".join(ps) + ");" in hdr

@@ -23,6 +23,11 @@ pytestmark = pytest.mark.gpu
 RTOL = 1e-10
 
 
+def g_params(cls):
+    """Parameter names of vlxb_computeCoulombGradient<cls>, in ABI order."""
+    return lib().g_params[cls]
+
+
 def close(got, exp):
     scale = float(np.abs(exp).max()) if exp.size else 0.0
     return float(np.abs(got - exp).max()) <= RTOL * scale + 1e-14 if exp.size else True
@@ -96,15 +101,11 @@ def test_gradient_argument_checks(system):
     n = len(rl.jlists["pd"].first)
     G = torch.zeros((6, n), dtype=torch.float64, device="cuda")
     args = gradient.grad_args(dl, "pdpd", G, 0, n - 1, s)  # stride below the entry count
-    vals = [args[p] for p in L_params("pdpd")]
+    vals = [args[p] for p in g_params("pdpd")]
     rc = getattr(lib().cdll, "vlxb_computeCoulombGradientPDPD")(*vals)
     assert rc == 1  # VLXB_EINVAL
     torch.cuda.synchronize()
     assert float(G.abs().max()) == 0.0
-
-
-def L_params(cls):
-    return lib().g_params[cls]
 
 
 def test_every_exchange_gradient_class_vs_oracle(system):
