@@ -73,3 +73,36 @@ def test_gradient_entry_points_declared_and_bound():
         ps = ABI.kg_params(cls)
         assert ps[:2] == ["double* grad_K", "uint64_t grad_stride"] and ps[2:] == ABI.k_params(cls)[1:]
         assert f"int vlxb_computeExchangeGradient{cls.upper()}(" + ", ".join(ps) + ");" in hdr
+
+
+def test_gradient_argument_checks_without_gpu():
+    """Checks the gradient entry points and the fold make before any device
+    call: a component stride beyond int64, no atoms, and empty lists."""
+    from vlxb._lib import Lib
+
+    L = Lib()
+    c = L.cdll
+    dummy = ctypes.c_double(0.0)
+    p = ctypes.addressof(dummy)  # never dereferenced: every call below returns before touching memory
+    huge = (1 << 63) + 5
+    # the fold: no atoms, stride past the int64 range
+    assert c.vlxb_pairGradientToAtoms(p, 0, None, p, p, 0, p, None) == 1
+    assert c.vlxb_pairGradientToAtoms(p, 1 << 62, None, p, p, 2, p, None) == 1
+    # stride beyond int64: rejected before any list is read
+    for cls, names, fn in (("ssss", L.g_params["ssss"], c.vlxb_computeCoulombGradientSSSS),
+                           ("ssss", L.kg_params["ssss"], c.vlxb_computeExchangeGradientSSSS)):
+        args = []
+        for n in names:
+            if n == "grad_stride":
+                args.append(huge)
+            elif n in ("eri_threshold", "omega") or n.endswith("_max_D"):
+                args.append(0.0)
+            elif n.endswith("_count") or n.endswith("_count_local") or n.startswith("pair_inds_count") or n == "naos":
+                args.append(1)
+            else:
+                args.append(p)
+        assert fn(*args) == 1, cls
+    # empty bra list: success, nothing to do
+    args = [p if n not in ("grad_stride", "eri_threshold") and "count" not in n else 0 for n in L.g_params["ssss"]]
+    args[L.g_params["ssss"].index("grad_stride")] = 1
+    assert c.vlxb_computeCoulombGradientSSSS(*args) == 0
