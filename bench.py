@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--serve-atoms", type=int, nargs=2, default=(5, 12), help="served leg: atom count range")
     ap.add_argument("--serve-iters", type=int, default=10, help="served leg: densities per request")
     ap.add_argument("--serve-rate", type=float, default=50.0, help="served leg: Poisson arrival rate (req/s)")
+    ap.add_argument("--gradient-cpu", action="store_true",
+                    help="only the CPU baseline of the nuclear gradients (oracle port, no GPU) and exit")
+    ap.add_argument("--gradient-atoms", type=int, default=10, help="--gradient-cpu: atoms of the molecule")
     return ap.parse_args()
 
 
@@ -629,8 +632,71 @@ def run_ours(args):
     return 0
 
 
+def run_gradient_cpu(args):
+    """CPU baseline of the nuclear gradients dE_J/dR and dE_K/dR.  The
+    reference has no gradient code, so this times the oracle's derivative
+    routines (a port: the Obara-Saika derivative relation on the oracle's
+    integrals, all host threads) on the molecule `python -m vlxb.gradbench`
+    times on the GPU: per class a seeded sample of bra rows (J) or (i, k) rows
+    (K), extrapolated to all rows.  Needs no GPU.  Prints one JSON line."""
+    from oracle import oracle
+    from vlxb import basis, lists
+
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    wl = basis.molecule_at_density(args.gradient_atoms, 30.0, 7)
+
+    def schwarz(la, lb, pd, P, Q):
+        out = np.zeros(len(P))
+        ia, ib = pd.info[la], pd.info[lb]
+        for t, (p, q) in enumerate(zip(P, Q)):
+            A, B = ia[2:5, p], ib[2:5, q]
+            I = oracle.eri_shell_quartet(la, lb, la, lb, ia[0, p], A, ib[0, q], B, ia[0, p], A, ib[0, q], B)
+            n = I.shape[0] * I.shape[1]
+            out[t] = np.sqrt(np.abs(np.diag(I.reshape(n, n))).max())
+        return out
+
+    rl = lists.build_lists(wl.mol, wl.D, wl.threshold, schwarz)
+    rng = np.random.default_rng(11)
+    LVv = lists.LV
+    est = {"J": 0.0, "K": 0.0}
+    rows_total = {"J": 0, "K": 0}
+    for cls in lists.j_classes():
+        if cls[:2] not in rl.jlists or cls[2:] not in rl.jlists:
+            continue
+        jab, jcd = rl.jlists[cls[:2]], rl.jlists[cls[2:]]
+        n = len(jab.first)
+        rows = np.sort(rng.choice(n, size=min(n, 2 * threads), replace=False)).astype(np.uint32)
+        t0 = time.perf_counter()
+        oracle.coulomb_grad(LVv[cls[0]], LVv[cls[1]], LVv[cls[2]], LVv[cls[3]], rl.pd.info, rl.pd.count, jcd.D,
+                            jab.Q, jcd.Q, jab.first, jab.second, jab.pdata, jcd.first, jcd.second, jcd.pdata,
+                            rl.threshold, rows=rows)
+        est["J"] += (time.perf_counter() - t0) * n / len(rows)
+        rows_total["J"] += len(rows)
+    for cls in lists.k_classes():
+        a, b, c, d = cls
+        if a + c not in rl.kpairs or a + b not in rl.kpartners or c + d not in rl.kpartners:
+            continue
+        kq, p1, p2 = rl.kpairs[a + c], rl.kpartners[a + b], rl.kpartners[c + d]
+        n = len(kq.pair_i)
+        rows = np.sort(rng.choice(n, size=min(n, 2 * threads), replace=False)).astype(np.uint32)
+        t0 = time.perf_counter()
+        oracle.exchange_grad(LVv[a], LVv[b], LVv[c], LVv[d], kq.pair_i, kq.pair_k, rl.pd.info, rl.pd.aoinds,
+                             rl.pd.count, rl.maxD[b + d], rl.D_AO, p1.Q, p2.Q, p1.Dinds, p2.Dinds, p1.displs,
+                             p2.displs, p1.counts, p2.counts, p1.pdata, p2.pdata, 0.0, rl.threshold, rows=rows)
+        est["K"] += (time.perf_counter() - t0) * n / len(rows)
+        rows_total["K"] += len(rows)
+    print(json.dumps({"metric": "nuclear-gradient time, CPU port (oracle)", "unit": "s",
+                      "workload": wl.name, "naos": wl.mol.naos, "dEJ_dR_s": round(est["J"], 2),
+                      "dEK_dR_s": round(est["K"], 2), "cores": threads, "kind": "port",
+                      "sample": f"{rows_total['J']} J bra rows and {rows_total['K']} K (i, k) rows "
+                                f"(2 x threads per class), extrapolated per class to all rows"}))
+    return 0
+
+
 def main():
     args = parse()
+    if args.gradient_cpu:
+        return run_gradient_cpu(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
