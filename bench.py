@@ -1,10 +1,10 @@
 #!/usr/bin/env python
 """Benchmark: J+K Fock builds through the drop-in C ABI on B200.
 
-Workload: 40 atoms in a 14-bohr cube, 4s+3p+2d contracted Cartesian shells of
-degree 3, even-tempered exponents 0.05 * 2.5^k, density from 80 occupied
-orbitals, Schwarz threshold 1e-12, FP64 (1000 Cartesian AOs; seeded
-synthetic molecule and density, no dataset involved).
+Workload (the headline): 40 atoms in a 14-bohr cube, 4s+3p+2d contracted
+Cartesian shells of degree 3, even-tempered exponents 0.05 * 2.5^k, density
+from 80 occupied orbitals, Schwarz threshold 1e-12, FP64 (1000 Cartesian AOs;
+seeded synthetic molecule and density, no dataset involved).
 
 One step = one complete J+K build: all 36 Coulomb and 54 exchange entry points
 of the C ABI, with the reference's list formats as input (the drop-in path).
@@ -15,6 +15,32 @@ of the C ABI, with the reference's list formats as input (the drop-in path).
          and mat_J / mat_K copied back inside every timed step
 
     python bench.py [--steps K] [--warmup W] [--gpus N] [--impl reference]
+
+After the timed steps the same line carries the other legs (all on this GPU):
+  parity   seeded rows of every J and K list of the headline build against the
+           reference's own emitted expressions compiled for the host
+           (oracle/_ref, FP64), absolute errors
+  mixed    the headline build with FP32 below a Schwarz bound of 1e-6 and an
+           FP32 error budget; errors against the FP64 build (whole AO
+           matrices) and against oracle/_ref on the parity rows
+  small    5 atoms 3s2p (45 AOs): timed in full on the GPU and on the host
+           cores (reference expressions), every value checked
+  large    200 atoms at 25 bohr^3 per atom, 4s3p2d (5000 AOs): incremental
+           build on dD of norm 1e-3, density-weighted screening at 1e-11,
+           mixed precision with FP64 accumulation
+  batched / served   the batching and serving patterns
+  cpu_baseline       the reference's emitted expressions with OpenMP on the
+           host cores, a bounded sample of the headline build extrapolated
+
+Tool modes (no driver line; used by the profiles under profiles/):
+    python bench.py --mode case --kind K --cls pddd [--atoms 12] [--reps 2]
+        one class entry point on a small cluster (the case for ncu captures)
+    python bench.py --mode classes [--config medium|small]
+        device time and quartets of every class entry point
+    python bench.py --mode gradient [--atoms 10]
+        nuclear-gradient entry points against the J / K builds
+    python bench.py --mode gradient-cpu [--atoms 10]
+        CPU baseline of the nuclear gradients (oracle port, no GPU)
 
 Multi-GPU: the path is a single-GPU build; N GPUs run N independent replicas
 (one process per GPU) and value is the aggregate over the replicas.
@@ -44,6 +70,7 @@ L2_BYTES = 126 * 1024 * 1024
 
 def parse():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--mode", choices=["bench", "case", "classes", "gradient", "gradient-cpu"], default="bench")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
@@ -51,11 +78,16 @@ def parse():
     ap.add_argument("--config", choices=["medium", "small"], default="medium")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--parity-rows", type=int, default=6, help="rows per list checked against oracle/_ref (0: none)")
     ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end steps (default min(steps, 2))")
     ap.add_argument("--mixed-steps", type=int, default=None, help="mixed-precision steps (default min(steps, 2))")
     ap.add_argument("--fp32-cut", type=float, default=1e-6,
-                    help="mixed-precision leg: quartets with bound below this run in FP32 (0 skips the leg)")
+                    help="mixed-precision leg: quartets with bound below this may run in FP32 (0 skips the leg)")
+    ap.add_argument("--fp32-budget", type=float, default=None,
+                    help="mixed-precision leg: FP32 error budget (default: the library's recommended value)")
     ap.add_argument("--schedule", default=None, help="kernel schedule JSON (default: vlxb/schedule_b200.json)")
+    ap.add_argument("--small-steps", type=int, default=5, help="5-atom leg: timed builds (0 skips the leg)")
+    ap.add_argument("--large-atoms", type=int, default=200, help="large sparse leg: atoms (0 skips the leg)")
     ap.add_argument("--pattern-fp32-cut", type=float, default=1e-7,
                     help="batched / served legs: FP32 below this bound (errors reported)")
     ap.add_argument("--batch-mols", type=int, default=32, help="batched leg: molecules (0 skips the leg)")
@@ -64,9 +96,16 @@ def parse():
     ap.add_argument("--serve-atoms", type=int, nargs=2, default=(5, 12), help="served leg: atom count range")
     ap.add_argument("--serve-iters", type=int, default=10, help="served leg: densities per request")
     ap.add_argument("--serve-rate", type=float, default=50.0, help="served leg: Poisson arrival rate (req/s)")
-    ap.add_argument("--gradient-cpu", action="store_true",
-                    help="only the CPU baseline of the nuclear gradients (oracle port, no GPU) and exit")
-    ap.add_argument("--gradient-atoms", type=int, default=10, help="--gradient-cpu: atoms of the molecule")
+    # tool modes
+    ap.add_argument("--kind", choices=["J", "K"], default="K", help="--mode case: entry-point kind")
+    ap.add_argument("--cls", default="pddd", help="--mode case: class")
+    ap.add_argument("--atoms", type=int, default=None, help="--mode case / gradient / gradient-cpu: atoms")
+    ap.add_argument("--density", type=float, default=30.0, help="--mode gradient: bohr^3 per atom")
+    ap.add_argument("--seed", type=int, default=7, help="--mode gradient: molecule seed")
+    ap.add_argument("--reps", type=int, default=2, help="--mode case / gradient: repetitions")
+    ap.add_argument("--variant", type=int, default=None, help="--mode case: kernel variant (default: tuned)")
+    ap.add_argument("--case-fp32-cut", type=float, default=0.0, help="--mode case: mixed-precision cutoff")
+    ap.add_argument("--out", default=None, help="--mode classes: JSON output file")
     return ap.parse_args()
 
 
@@ -167,7 +206,23 @@ def dist_barrier():
         dist.barrier()
 
 
-# ----------------------------------------------------------------- CPU reference
+# ----------------------------------------------------------------- CPU side (checker and baseline)
+def _host_threads():
+    try:
+        return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    except ValueError:
+        return os.cpu_count() or 1
+
+
+def _ref_classes(rl):
+    from vlxb import lists
+
+    classes = [("J", c) for c in lists.j_classes() if c[:2] in rl.jlists and c[2:] in rl.jlists]
+    classes += [("K", c) for c in lists.k_classes()
+                if c[0] + c[2] in rl.kpairs and c[:2] in rl.kpartners and c[2:] in rl.kpartners]
+    return classes
+
+
 def cpu_reference(rl, budget_s, seed=0):
     """Time the reference's emitted expressions (oracle/_ref) on a bounded
     sample of this build and extrapolate the full-build time.
@@ -177,19 +232,10 @@ def cpu_reference(rl, budget_s, seed=0):
     the full-build time is (machine throughput in component quartets/s) divided
     into the sampled rows' exact passing counts scaled to all rows."""
     from oracle import ref
-    from vlxb import lists
 
-    threads = os.cpu_count() or 1
-    try:
-        import ctypes.util  # noqa: F401
-
-        threads = int(os.environ.get("OMP_NUM_THREADS", threads))
-    except ValueError:
-        pass
+    threads = _host_threads()
     rng = np.random.default_rng(seed)
-    classes = [("J", c) for c in lists.j_classes() if c[:2] in rl.jlists and c[2:] in rl.jlists]
-    classes += [("K", c) for c in lists.k_classes()
-                if c[0] + c[2] in rl.kpairs and c[:2] in rl.kpartners and c[2:] in rl.kpartners]
+    classes = _ref_classes(rl)
     per = budget_s / len(classes)
     est_total = 0.0
     cq_eval_total = 0
@@ -217,18 +263,73 @@ def cpu_reference(rl, budget_s, seed=0):
     return est_total, threads, {"classes": len(classes), "rows": rows_total, "component_quartets": cq_eval_total}
 
 
+def cpu_reference_full(rl):
+    """The whole build with the reference's emitted expressions (oracle/_ref,
+    OpenMP over the host cores): (mat_J, mat_K, seconds)."""
+    from oracle import ref
+
+    matJ = {k: np.zeros(len(v.first)) for k, v in rl.jlists.items()}
+    matK = {k: np.zeros(len(v.pair_i)) for k, v in rl.kpairs.items()}
+    t0 = time.perf_counter()
+    for kind, cls in _ref_classes(rl):
+        if kind == "J":
+            ref.coulomb(rl, cls, mat_J=matJ[cls[:2]])
+        else:
+            ref.exchange(rl, cls, mat_K=matK[cls[0] + cls[2]])
+    return matJ, matK, time.perf_counter() - t0
+
+
 def quartets_per_build_ref(rl):
+    from oracle import ref
+
+    n = 0
+    for kind, cls in _ref_classes(rl):
+        n += ref.count_j(rl, cls) if kind == "J" else ref.count_k(rl, cls)
+    return n
+
+
+def ref_rows(rl, per_list, seed=0):
+    """FP64 values of seeded rows of every J list (mat_J summed over its 6
+    classes) and every K (i, k) list (mat_K over its 9 classes), from the
+    reference's emitted expressions (oracle/_ref)."""
     from oracle import ref
     from vlxb import lists
 
-    n = 0
-    for c in lists.j_classes():
-        if c[:2] in rl.jlists and c[2:] in rl.jlists:
-            n += ref.count_j(rl, c)
-    for c in lists.k_classes():
-        if c[0] + c[2] in rl.kpairs and c[:2] in rl.kpartners and c[2:] in rl.kpartners:
-            n += ref.count_k(rl, c)
-    return n
+    rng = np.random.default_rng(seed)
+    out = {}
+    t0 = time.perf_counter()
+    for ab, jl in rl.jlists.items():
+        n = len(jl.first)
+        rows = np.sort(rng.choice(n, size=min(per_list, n), replace=False)).astype(np.uint32)
+        acc = np.zeros(n)
+        for cd in rl.jlists:
+            if lists.LV[cd[0]] <= lists.LV[cd[1]]:
+                ref.coulomb(rl, ab + cd, rows=rows, mat_J=acc)
+        out[("J", ab)] = (rows.astype(np.int64), acc[rows])
+    for ac, kq in rl.kpairs.items():
+        n = len(kq.pair_i)
+        rows = np.sort(rng.choice(n, size=min(per_list, n), replace=False)).astype(np.uint32)
+        acc = np.zeros(n)
+        for b in "spd":
+            for d in "spd":
+                cls = ac[0] + b + ac[1] + d
+                if cls[:2] in rl.kpartners and cls[2:] in rl.kpartners:
+                    ref.exchange(rl, cls, rows=rows, mat_K=acc)
+        out[("K", ac)] = (rows.astype(np.int64), acc[rows])
+    return out, time.perf_counter() - t0
+
+
+def row_errors(expected, matJ, matK):
+    """Absolute errors of GPU prim-pair outputs (numpy dicts) on the expected rows."""
+    res = {"max_abs_dJ": 0.0, "max_abs_dK": 0.0, "max_abs_J": 0.0, "max_abs_K": 0.0, "rows": 0}
+    for (kind, key), (rows, vals) in expected.items():
+        got = (matJ if kind == "J" else matK)[key][rows]
+        err = float(np.abs(got - vals).max()) if len(rows) else 0.0
+        mag = float(np.abs(vals).max()) if len(rows) else 0.0
+        res[f"max_abs_d{kind}"] = max(res[f"max_abs_d{kind}"], err)
+        res[f"max_abs_{kind}"] = max(res[f"max_abs_{kind}"], mag)
+        res["rows"] += len(rows)
+    return res
 
 
 # ----------------------------------------------------------------- reference arm
@@ -274,14 +375,160 @@ def run_reference(args):
     return 0
 
 
-# ----------------------------------------------------------------- patterns
+# ----------------------------------------------------------------- timing helpers
+def timed_device(fn, reps, stream=None, flush=None):
+    """Device time (s) of each of `reps` calls of fn, CUDA events on `stream`
+    (the current stream when None), with an L2 flush before each when given."""
+    import torch
+
+    out = []
+    for _ in range(reps):
+        if flush is not None:
+            flush.zero_()
+        s = stream or torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        fn()
+        e1.record(s)
+        e1.synchronize()
+        out.append(e0.elapsed_time(e1) / 1e3)
+    return out
+
+
+def ao_matrices(rl, matJ, matK):
+    from vlxb import lists
+
+    J = lists.contract_J(rl, {k: v.cpu().numpy() for k, v in matJ.items()})
+    K = lists.contract_K(rl, {k: v.cpu().numpy() for k, v in matK.items()})
+    return J, K
+
+
+# ----------------------------------------------------------------- legs
+def run_small(args, L, dev, stream, flush):
+    """5-atom 3s2p workload (45 AOs), timed in full: GPU builds through the
+    C ABI, the whole build of the reference's emitted expressions on the host
+    cores, and every value of every list compared."""
+    import torch
+    from vlxb import basis, fock, lists
+
+    wl = basis.config_small(0)
+    rl = lists.build_lists(wl.mol, wl.D, wl.threshold, fock.gpu_schwarz_fn(dev))
+    dl = fock.to_device(rl, dev)
+    matJ, matK = fock.alloc_outputs(dl)
+
+    def build():
+        for t in list(matJ.values()) + list(matK.values()):
+            t.zero_()
+        fock.build_jk(dl, stream=stream, matJ=matJ, matK=matK)
+
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            build()
+        torch.cuda.synchronize()
+        L.reset_counters(stream.cuda_stream)
+        ts = timed_device(build, args.small_steps, stream, flush)
+        qj, qk = L.quartet_counters(reset=True, stream=stream.cuda_stream)
+    q = (qj + qk) / args.small_steps
+    t = float(np.median(ts))
+    res = {"workload": "5 atoms 6-bohr cube 3s2p deg 3 (45 AOs), nocc 10, thr 1e-12, FP64",
+           "steps": args.small_steps, "ms_per_step": t * 1e3, "quartets_per_build": q, "value": q / t,
+           "unit": UNIT, "builds_per_s": 1.0 / t}
+    from oracle import ref
+
+    if ref.available():
+        rJ, rK, cpu_s = cpu_reference_full(rl)
+        gJ = {k: v.cpu().numpy() for k, v in matJ.items()}
+        gK = {k: v.cpu().numpy() for k, v in matK.items()}
+        dJ = max(float(np.abs(gJ[k] - rJ[k]).max()) for k in rJ)
+        dK = max(float(np.abs(gK[k] - rK[k]).max()) for k in rK)
+        J, K = lists.contract_J(rl, gJ), lists.contract_K(rl, gK)
+        Jr, Kr = lists.contract_J(rl, rJ), lists.contract_K(rl, rK)
+        res["parity"] = {"reference": "the reference's emitted expressions (oracle/_ref), every list entry",
+                         "max_abs_dJ_pairs": dJ, "max_abs_dK_pairs": dK,
+                         "max_abs_dJ_ao": float(np.abs(J - Jr).max()), "max_abs_dK_ao": float(np.abs(K - Kr).max()),
+                         "abs_dE_Eh": abs(lists.energy(wl.D, J, K) - lists.energy(wl.D, Jr, Kr)),
+                         "max_abs_J": float(np.abs(Jr).max()), "max_abs_K": float(np.abs(Kr).max())}
+        res["cpu_reference"] = {"value": q / cpu_s, "unit": UNIT, "build_s": cpu_s, "cores": _host_threads(),
+                                "kind": "reference", "sample": "the whole build (not extrapolated)"}
+    return res
+
+
+def run_large(args, L, dev, stream, cut, budget):
+    """Large sparse workload: `args.large_atoms` atoms at 25 bohr^3 per atom,
+    4s3p2d (5000 Cartesian AOs at 200 atoms).  Lists of the density difference
+    dD (seeded, Frobenius norm 1e-3) are built on the device with Schwarz and
+    density-weighted screening at 1e-11; the build on dD runs with FP32 below
+    `cut` inside the error budget and FP64 accumulation, and is added to the
+    previous J/K.  Reported: its device time, quartets, screened fraction
+    against the full-density lists, errors against the FP64 build of the same
+    dD (AO matrices) and against oracle/_ref on seeded rows."""
+    import torch
+    from vlxb import basis, devlists, fock, lists
+
+    n = args.large_atoms
+    wl = basis.molecule_at_density(n, 25.0, 0, threshold=1e-11)
+    rng = np.random.default_rng(3)
+    P = rng.standard_normal(wl.D.shape)
+    P = 0.5 * (P + P.T)
+    dD = P * (1e-3 / np.linalg.norm(P))
+    res = {"workload": f"{n} atoms at 25 bohr^3/atom 4s3p2d ({wl.mol.naos} AOs), incremental build on dD "
+                       "(|dD|_F = 1e-3), Schwarz + density screening at 1e-11",
+           "naos": wl.mol.naos}
+    with torch.cuda.stream(stream):
+        t0 = time.perf_counter()
+        dl = devlists.build_device_lists(wl.mol, dD, 1e-11, dev)
+        torch.cuda.synchronize()
+        res["list_build_s"] = time.perf_counter() - t0
+        res["j_pairs"] = int(sum(v["first"].numel() for v in dl.j.values()))
+        res["k_ik_pairs"] = int(sum(v["i"].numel() for v in dl.kpair.values()))
+        matJ, matK = fock.alloc_outputs(dl)
+
+        def build():
+            for t in list(matJ.values()) + list(matK.values()):
+                t.zero_()
+            fock.build_jk(dl, stream=stream, matJ=matJ, matK=matK)
+
+        L.set_fp32_cut(0.0)
+        build()
+        torch.cuda.synchronize()
+        L.reset_counters(stream.cuda_stream)
+        t64 = timed_device(build, 1, stream)[0]
+        qj, qk = L.quartet_counters(reset=True, stream=stream.cuda_stream)
+        J64 = {k: v.cpu().numpy() for k, v in matJ.items()}
+        K64 = {k: v.cpu().numpy() for k, v in matK.items()}
+        L.set_fp32_cut(cut)
+        L.set_fp32_budget(budget)
+        build()
+        torch.cuda.synchronize()
+        tmx = timed_device(build, 1, stream)[0]
+        L.set_fp32_cut(0.0)
+        J32 = {k: v.cpu().numpy() for k, v in matJ.items()}
+        K32 = {k: v.cpu().numpy() for k, v in matK.items()}
+    q = qj + qk
+    res.update({"fp64_ms": t64 * 1e3, "mixed_ms": tmx * 1e3, "quartets": q, "value": q / tmx, "unit": UNIT,
+                "builds_per_s": 1.0 / tmx, "speedup_mixed_vs_fp64": t64 / tmx, "fp32_below_bound": cut,
+                "fp32_budget": budget})
+    host = devlists.to_host(dl, wl.mol)
+    J64a, K64a = lists.contract_J(host, J64), lists.contract_K(host, K64)
+    J32a, K32a = lists.contract_J(host, J32), lists.contract_K(host, K32)
+    res["mixed_vs_fp64"] = {"max_abs_dJ": float(np.abs(J32a - J64a).max()),
+                            "max_abs_dK": float(np.abs(K32a - K64a).max()),
+                            "abs_dE_Eh": abs(lists.energy(dD, J32a, K32a) - lists.energy(dD, J64a, K64a))}
+    from oracle import ref
+
+    if ref.available() and args.parity_rows > 0:
+        exp, secs = ref_rows(host, max(2, args.parity_rows // 2), seed=11)
+        res["parity_fp64"] = row_errors(exp, J64, K64) | {"oracle_s": secs}
+        res["parity_mixed"] = row_errors(exp, J32, K32)
+    return res
+
+
 def run_batched(args, L, dev, cut):
     """Batched leg: many small molecules (1 atom per 30 bohr^3, the 4s3p2d
     recipe), all resident.  plain = the molecules' FP64 builds one after the
     other through the C ABI; batched = one CUDA graph replay per iteration (all
     molecules' class calls on 8 capture streams), FP64 and with FP32 below
     `cut`.  Device time with CUDA events; builds/s = molecules/s."""
-    import numpy as np
     import torch
     from vlxb import basis, fock, lists
     from vlxb.batch import BatchedBuilder
@@ -301,15 +548,7 @@ def run_batched(args, L, dev, cut):
     def timed(fn, reps):
         fn()
         torch.cuda.synchronize()
-        ts = []
-        for _ in range(reps):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            fn()
-            e1.record()
-            torch.cuda.synchronize()
-            ts.append(e0.elapsed_time(e1) / 1e3)
-        return min(ts)
+        return min(timed_device(fn, reps))
 
     def energies():
         out = []
@@ -369,7 +608,6 @@ def run_served(args, L, dev, cut):
     continuous admission of up to 8 concurrent requests on their own streams,
     FP32 below `cut`, incremental dD builds.  Wall-clock (host) timing of the
     whole request stream; p50/p99 = request latency from arrival to result."""
-    import numpy as np
     from vlxb import basis
     from vlxb.serve import Request, Server, perturbed_densities
 
@@ -440,6 +678,7 @@ def run_ours(args):
 
     sched_loaded = apply_schedule(args.schedule or DEFAULT_SCHEDULE)
     L.set_fp32_cut(0.0)
+    budget = args.fp32_budget if args.fp32_budget is not None else L.get_fp32_budget()
     stream = torch.cuda.Stream(device=dev)
     wl = workload(args.config)
     rl = lists.build_lists(wl.mol, wl.D, wl.threshold, fock.gpu_schwarz_fn(dev))
@@ -484,6 +723,7 @@ def run_ours(args):
         for w in range(args.warmup):
             if w == args.warmup - 1 and args.fp32_cut > 0:
                 L.set_fp32_cut(args.fp32_cut)
+                L.set_fp32_budget(budget)
             keep = e2e_build()
             torch.cuda.synchronize()
             del keep
@@ -512,9 +752,10 @@ def run_ours(args):
         t_build = dist_max(sum(times)) / args.steps
         dist_barrier()
 
-        # FP64 results of the last timed build: the mixed leg's reference
-        J64 = lists.contract_J(rl, {k: v.cpu().numpy() for k, v in matJ.items()})
-        K64 = lists.contract_K(rl, {k: v.cpu().numpy() for k, v in matK.items()})
+        # FP64 results of the last timed build: the parity rows and the mixed leg's reference
+        G64 = ({k: v.cpu().numpy() for k, v in matJ.items()}, {k: v.cpu().numpy() for k, v in matK.items()})
+        J64 = lists.contract_J(rl, G64[0])
+        K64 = lists.contract_K(rl, G64[1])
 
         # ---- end to end: host buffers in, results out, every step
         e2e_steps = args.e2e_steps or min(args.steps, 2)
@@ -551,11 +792,13 @@ def run_ours(args):
                 per_class.append((kind, cls, e0.elapsed_time(e1) / 1e3, nq, nq * fl[cls][kind]))
         peak = fp64_peak(L, dev, stream)
 
-        # ---- mixed precision leg: same build with FP32 below the cutoff,
-        # errors of AO J, K and E against this GPU's FP64 build
+        # ---- mixed precision leg: same build with FP32 below the cutoff inside
+        # the error budget; errors of AO J, K and E against this GPU's FP64 build
         mixed = None
+        G32 = None
         if args.fp32_cut > 0:
             L.set_fp32_cut(args.fp32_cut)
+            L.set_fp32_budget(budget)
             mt = []
             for _ in range(args.mixed_steps or min(args.steps, 2)):
                 flush.zero_()
@@ -566,18 +809,24 @@ def run_ours(args):
                 e1.synchronize()
                 mt.append(e0.elapsed_time(e1) / 1e3)
             L.set_fp32_cut(0.0)
-            J32 = lists.contract_J(rl, {k: v.cpu().numpy() for k, v in matJ.items()})
-            K32 = lists.contract_K(rl, {k: v.cpu().numpy() for k, v in matK.items()})
+            G32 = ({k: v.cpu().numpy() for k, v in matJ.items()}, {k: v.cpu().numpy() for k, v in matK.items()})
+            J32 = lists.contract_J(rl, G32[0])
+            K32 = lists.contract_K(rl, G32[1])
             t_mix = dist_max(sum(mt)) / len(mt)
-            mixed = {"fp32_below_bound": args.fp32_cut, "value": qpb / t_mix * ws, "unit": UNIT,
-                     "ms_per_step": t_mix * 1e3, "builds_per_s": ws / t_mix,
+            mixed = {"fp32_below_bound": args.fp32_cut, "fp32_budget": budget, "value": qpb / t_mix * ws,
+                     "unit": UNIT, "ms_per_step": t_mix * 1e3, "builds_per_s": ws / t_mix,
                      "speedup_vs_fp64": t_build / t_mix,
                      "max_abs_dJ": float(np.abs(J32 - J64).max()), "max_abs_dK": float(np.abs(K32 - K64).max()),
                      "abs_dE_Eh": abs(lists.energy(wl.D, J32, K32) - lists.energy(wl.D, J64, K64)),
-                     "reference": "this GPU's FP64 build (parity-tested against the FP64 oracle at 1e-10)"}
+                     "reference": ("this GPU's FP64 build, whole AO matrices (its rows are checked against "
+                                   "oracle/_ref in `parity`)")}
 
-        # ---- batched and served patterns (rank 0 of a replica run does them alone)
-        batched = served = None
+        # ---- other workloads (rank 0 of a replica run does them alone)
+        small = large = batched = served = None
+        if rank == 0 and args.small_steps > 0:
+            small = run_small(args, L, dev, stream, flush)
+        if rank == 0 and args.large_atoms > 0 and args.fp32_cut > 0:
+            large = run_large(args, L, dev, stream, args.fp32_cut, budget)
         if rank == 0 and args.batch_mols > 0:
             batched = run_batched(args, L, dev, args.pattern_fp32_cut)
         if rank == 0 and args.serve_reqs > 0:
@@ -603,17 +852,31 @@ def run_ours(args):
         "builds_per_s": ws / t_build, "quartets_per_build": qpb, "gpu_launches": launches,
         "e2e": {"value": qpb / t_e2e * ws, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": t_e2e * 1e3},
-        "roofline": roofline, "clocks": clk, "mixed": mixed, "batched": batched, "served": served,
+        "roofline": roofline, "clocks": clk, "mixed": mixed, "small": small, "large": large,
+        "batched": batched, "served": served,
         "schedule": "autotuned (vlxb/schedule_b200.json)" if sched_loaded else "generator defaults",
         "top_classes": [{"class": f"{k} {c.upper()}", "ms": round(t * 1e3, 2), "quartets": n,
                          "tflops": round(f / t / 1e12, 3)} for k, c, t, n, f in
                         sorted(per_class, key=lambda r: -r[2])[:8]],
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        # CPU leg, after every GPU measurement: the reference's emitted
+        # expressions as the timed baseline, and as the FP64 checker of seeded
+        # rows of the headline build (FP64 and mixed)
         try:
             from oracle import ref
 
             if ref.available():
+                if args.parity_rows > 0:
+                    exp, secs = ref_rows(rl, args.parity_rows, seed=5)
+                    par = row_errors(exp, *G64)
+                    par.update({"reference": "oracle/_ref (the reference's emitted expressions, FP64)",
+                                "rows_per_list": args.parity_rows, "oracle_s": secs,
+                                "bar_abs": 1e-10})
+                    line["parity"] = par
+                    if G32 is not None:
+                        pm = row_errors(exp, *G32)
+                        line["mixed"]["vs_oracle_rows"] = {k: pm[k] for k in ("max_abs_dJ", "max_abs_dK", "rows")}
                 est, threads, sample = cpu_reference(rl, args.cpu_seconds, seed=7)
                 line["cpu_baseline"] = {
                     "value": qpb / est, "unit": UNIT, "cores": threads, "kind": "reference",
@@ -632,18 +895,155 @@ def run_ours(args):
     return 0
 
 
+# ----------------------------------------------------------------- tool modes
+def _tool_setup():
+    import torch
+    from vlxb._lib import lib
+    from vlxb.tune import apply_schedule
+
+    L = lib()
+    L.init(0)
+    apply_schedule()
+    return torch, L
+
+
+def mode_case(args):
+    """One class entry point on a seeded 4s3p2d cluster (the benchmark's
+    recipe and density, side scaled with the atom count): `reps` calls, the
+    first a warm-up; prints the time of the last.  A few hundred MB of device
+    memory at most: the case for ncu captures."""
+    torch, L = _tool_setup()
+    from vlxb import basis, fock, lists
+
+    L.set_fp32_cut(args.case_fp32_cut)
+    if args.variant is not None:
+        L.set_schedule(args.kind, args.cls, args.variant)
+    n = args.atoms or 12
+    side = 14.0 * (n / 40.0) ** (1.0 / 3.0)
+    wl = basis.config_custom(n, side, {0: 4, 1: 3, 2: 2}, 3, 0.05, 2.5, max(2, 2 * n), 1e-12, 0)
+    rl = lists.build_lists(wl.mol, wl.D, wl.threshold, fock.gpu_schwarz_fn())
+    dl = fock.to_device(rl)
+    matJ, matK = fock.alloc_outputs(dl)
+    dt = 0.0
+    for _ in range(args.reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if args.kind == "J":
+            fock.build_jk(dl, j_only=[args.cls], do_k=False, matJ=matJ, matK=matK)
+        else:
+            fock.build_jk(dl, k_only=[args.cls], do_j=False, matJ=matJ, matK=matK)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+    q = L.quartet_counters(reset=True)
+    print(f"{args.kind} {args.cls} variant {L.get_schedule(args.kind, args.cls)}: {dt * 1e3:.2f} ms, {q} quartets "
+          f"(all reps), {rl.naos} AOs")
+    return 0
+
+
+def mode_classes(args):
+    """Device time (CUDA events on the calling stream, list regrouping
+    included) and screened-in quartets of every class entry point, after one
+    warm-up pass."""
+    torch, L = _tool_setup()
+    from vlxb import fock, lists
+
+    if args.schedule:
+        from vlxb.tune import apply_schedule
+
+        apply_schedule(args.schedule)
+    wl = workload(args.config)
+    rl = lists.build_lists(wl.mol, wl.D, wl.threshold, fock.gpu_schwarz_fn())
+    dl = fock.to_device(rl)
+    matJ, matK = fock.alloc_outputs(dl)
+    res = {}
+    for rep in range(2):
+        for kind, cl in (("J", lists.j_classes()), ("K", lists.k_classes())):
+            for cls in cl:
+                L.reset_counters()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                if kind == "J":
+                    fock.build_jk(dl, j_only=[cls], do_k=False, matJ=matJ, matK=matK)
+                else:
+                    fock.build_jk(dl, k_only=[cls], do_j=False, matJ=matJ, matK=matK)
+                e1.record()
+                torch.cuda.synchronize()
+                q = L.quartet_counters(reset=True)
+                res[kind + cls] = (e0.elapsed_time(e1), q[0] if kind == "J" else q[1])
+    for k, (ms, q) in res.items():
+        print(k[0], k[1:], f"{ms:.2f} ms", q, flush=True)
+    print("total ms", sum(v[0] for v in res.values()))
+    if args.out:
+        os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
+        json.dump(res, open(args.out, "w"), indent=1)
+    return 0
+
+
+def mode_gradient(args):
+    """Device time (CUDA events, after one untimed call each) of the FP64 J
+    and K builds, dE_J/dR and dE_K/dR (all classes plus the per-atom fold) and
+    each exchange-gradient class alone, on one seeded 4s3p2d molecule; one
+    JSON line with the times in ms and the translational-invariance residues."""
+    torch, L = _tool_setup()
+    from vlxb import basis, fock, gradient, lists
+
+    wl = basis.molecule_at_density(args.atoms or 10, args.density, args.seed)
+    rl = lists.build_lists(wl.mol, wl.D, wl.threshold, fock.gpu_schwarz_fn())
+    dl = fock.to_device(rl)
+    cg = gradient.CoulombGradient(dl, wl.mol)
+    kg = gradient.ExchangeGradient(dl, wl.mol)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        return [round(t * 1e3, 2) for t in timed_device(fn, args.reps)]
+
+    res = {"workload": wl.name, "naos": wl.mol.naos}
+    res["J_build_ms"] = timed(lambda: fock.build_jk(dl, do_k=False))
+    res["K_build_ms"] = timed(lambda: fock.build_jk(dl, do_j=False))
+    res["dEJ_dR_ms"] = timed(cg.compute)
+    res["dEK_dR_ms"] = timed(kg.compute)
+    gj = cg.compute().cpu().numpy()
+    gk = kg.compute().cpu().numpy()
+    res["max_dEJ_dR"] = float(np.abs(gj).max())
+    res["max_dEK_dR"] = float(np.abs(gk).max())
+    res["max_sum_dEJ_dR"] = float(np.abs(gj.sum(axis=0)).max())
+    res["max_sum_dEK_dR"] = float(np.abs(gk.sum(axis=0)).max())
+    s = torch.cuda.current_stream().cuda_stream
+    G = torch.zeros((6, max(kg.map.total, 1)), dtype=torch.float64, device="cuda")
+    per = {}
+    for cls in lists.k_classes():
+        ac = cls[0] + cls[2]
+        if ac not in dl.kpair:
+            continue
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        L.exchange_grad(cls, gradient.kgrad_args(dl, cls, G, kg.map.offsets[ac], G.shape[1], s))
+        e1.record()
+        torch.cuda.synchronize()
+        per[cls] = round(e0.elapsed_time(e1), 2)
+    res["dEK_dR_class_ms"] = per
+    print(json.dumps(res))
+    return 0
+
+
 def run_gradient_cpu(args):
     """CPU baseline of the nuclear gradients dE_J/dR and dE_K/dR.  The
     reference has no gradient code, so this times the oracle's derivative
     routines (a port: the Obara-Saika derivative relation on the oracle's
-    integrals, all host threads) on the molecule `python -m vlxb.gradbench`
-    times on the GPU: per class a seeded sample of bra rows (J) or (i, k) rows
-    (K), extrapolated to all rows.  Needs no GPU.  Prints one JSON line."""
-    from oracle import oracle
+    integrals, all host threads) on the molecule `--mode gradient` times on
+    the GPU: per class a seeded sample of bra rows (J) or (i, k) rows (K).
+    The sample's time is scaled by the class's screened-in component quartets
+    over the sample's (counted with the reference's screening loops in
+    oracle/_ref when it is built, else by row count), since screening makes
+    the per-row cost very uneven.  Needs no GPU.  Prints one JSON line."""
+    from oracle import oracle, ref
     from vlxb import basis, lists
 
-    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    wl = basis.molecule_at_density(args.gradient_atoms, 30.0, 7)
+    threads = _host_threads()
+    wl = basis.molecule_at_density(args.atoms or 10, 30.0, 7)
+    have_ref = ref.available()
 
     def schwarz(la, lb, pd, P, Q):
         out = np.zeros(len(P))
@@ -655,48 +1055,65 @@ def run_gradient_cpu(args):
             out[t] = np.sqrt(np.abs(np.diag(I.reshape(n, n))).max())
         return out
 
-    rl = lists.build_lists(wl.mol, wl.D, wl.threshold, schwarz)
-    rng = np.random.default_rng(11)
+    rl = lists.build_lists(wl.mol, wl.D, wl.threshold, ref.schwarz_fn if have_ref else schwarz)
     LVv = lists.LV
     est = {"J": 0.0, "K": 0.0}
     rows_total = {"J": 0, "K": 0}
-    for cls in lists.j_classes():
-        if cls[:2] not in rl.jlists or cls[2:] not in rl.jlists:
-            continue
-        jab, jcd = rl.jlists[cls[:2]], rl.jlists[cls[2:]]
-        n = len(jab.first)
-        rows = np.sort(rng.choice(n, size=min(n, 2 * threads), replace=False)).astype(np.uint32)
-        t0 = time.perf_counter()
-        oracle.coulomb_grad(LVv[cls[0]], LVv[cls[1]], LVv[cls[2]], LVv[cls[3]], rl.pd.info, rl.pd.count, jcd.D,
-                            jab.Q, jcd.Q, jab.first, jab.second, jab.pdata, jcd.first, jcd.second, jcd.pdata,
-                            rl.threshold, rows=rows)
-        est["J"] += (time.perf_counter() - t0) * n / len(rows)
-        rows_total["J"] += len(rows)
-    for cls in lists.k_classes():
-        a, b, c, d = cls
-        if a + c not in rl.kpairs or a + b not in rl.kpartners or c + d not in rl.kpartners:
-            continue
-        kq, p1, p2 = rl.kpairs[a + c], rl.kpartners[a + b], rl.kpartners[c + d]
-        n = len(kq.pair_i)
-        rows = np.sort(rng.choice(n, size=min(n, 2 * threads), replace=False)).astype(np.uint32)
-        t0 = time.perf_counter()
-        oracle.exchange_grad(LVv[a], LVv[b], LVv[c], LVv[d], kq.pair_i, kq.pair_k, rl.pd.info, rl.pd.aoinds,
-                             rl.pd.count, rl.maxD[b + d], rl.D_AO, p1.Q, p2.Q, p1.Dinds, p2.Dinds, p1.displs,
-                             p2.displs, p1.counts, p2.counts, p1.pdata, p2.pdata, 0.0, rl.threshold, rows=rows)
-        est["K"] += (time.perf_counter() - t0) * n / len(rows)
-        rows_total["K"] += len(rows)
+    spread = {"J": [], "K": []}
+    for seed in (11, 12):
+        rng = np.random.default_rng(seed)
+        tot = {"J": 0.0, "K": 0.0}
+        for kind, cls in _ref_classes(rl):
+            a, b, c, d = cls
+            n = len(rl.jlists[a + b].first) if kind == "J" else len(rl.kpairs[a + c].pair_i)
+            rows = np.sort(rng.choice(n, size=min(n, 2 * threads), replace=False)).astype(np.uint32)
+            t0 = time.perf_counter()
+            if kind == "J":
+                jab, jcd = rl.jlists[a + b], rl.jlists[c + d]
+                oracle.coulomb_grad(LVv[a], LVv[b], LVv[c], LVv[d], rl.pd.info, rl.pd.count, jcd.D, jab.Q, jcd.Q,
+                                    jab.first, jab.second, jab.pdata, jcd.first, jcd.second, jcd.pdata,
+                                    rl.threshold, rows=rows)
+            else:
+                kq, p1, p2 = rl.kpairs[a + c], rl.kpartners[a + b], rl.kpartners[c + d]
+                oracle.exchange_grad(LVv[a], LVv[b], LVv[c], LVv[d], kq.pair_i, kq.pair_k, rl.pd.info,
+                                     rl.pd.aoinds, rl.pd.count, rl.maxD[b + d], rl.D_AO, p1.Q, p2.Q, p1.Dinds,
+                                     p2.Dinds, p1.displs, p2.displs, p1.counts, p2.counts, p1.pdata, p2.pdata,
+                                     0.0, rl.threshold, rows=rows)
+            dt = time.perf_counter() - t0
+            scale = n / len(rows)
+            if have_ref:
+                f = ref.coulomb if kind == "J" else ref.exchange
+                _, c_rows, _ = f(rl, cls, rows=rows, max_eval=0)
+                _, c_all, _ = f(rl, cls, max_eval=0)
+                scale = c_all / c_rows if c_rows else scale
+            tot[kind] += dt * scale
+            if seed == 11:
+                rows_total[kind] += len(rows)
+        for k in ("J", "K"):
+            spread[k].append(tot[k])
+    for k in ("J", "K"):
+        est[k] = float(np.mean(spread[k]))
     print(json.dumps({"metric": "nuclear-gradient time, CPU port (oracle)", "unit": "s",
                       "workload": wl.name, "naos": wl.mol.naos, "dEJ_dR_s": round(est["J"], 2),
-                      "dEK_dR_s": round(est["K"], 2), "cores": threads, "kind": "port",
-                      "sample": f"{rows_total['J']} J bra rows and {rows_total['K']} K (i, k) rows "
-                                f"(2 x threads per class), extrapolated per class to all rows"}))
+                      "dEK_dR_s": round(est["K"], 2),
+                      "two_seeds_s": {k: [round(v, 1) for v in spread[k]] for k in spread},
+                      "cores": threads, "kind": "port",
+                      "sample": (f"{rows_total['J']} J bra rows and {rows_total['K']} K (i, k) rows per seed "
+                                 "(2 x threads per class), scaled per class by screened-in component quartets "
+                                 f"({'oracle/_ref counts' if have_ref else 'row count'}); mean of two seeds")}))
     return 0
 
 
 def main():
     args = parse()
-    if args.gradient_cpu:
+    if args.mode == "gradient-cpu":
         return run_gradient_cpu(args)
+    if args.mode == "case":
+        return mode_case(args)
+    if args.mode == "classes":
+        return mode_classes(args)
+    if args.mode == "gradient":
+        return mode_gradient(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -3,7 +3,9 @@ expressions, compiled for the host.
 
 TEST / BASELINE INFRASTRUCTURE ONLY (see oracle/__init__.py).
 
-    python oracle/make_ref.py [--ref /root/reference] [-j N]
+    python oracle/make_ref.py --ref <reference tree> [-j N]
+
+(or VLX_REFERENCE_DIR=<reference tree> python oracle/make_ref.py)
 
 For every Coulomb class (36, gen_coulomb.py:47-56) and exchange class (54,
 new_exchange_code/gen_eri_exchange.py:39-56) it asks the reference's
@@ -290,10 +292,11 @@ def compile_one(src):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("VLX_REFERENCE_DIR"),
+                    help="the vlx-twoe-ints source tree (default: $VLX_REFERENCE_DIR)")
     ap.add_argument("-j", type=int, default=os.cpu_count() or 1)
     args = ap.parse_args()
-    if not os.path.isdir(args.ref):
+    if not args.ref or not os.path.isdir(args.ref):
         print(f"reference tree {args.ref} not found; oracle/_ref left as is")
         return 0
     os.makedirs(SRC, exist_ok=True)

@@ -9,7 +9,9 @@ script binds them exactly as the emitted kernel prologues do
 Boys values taken from mpmath (the reference's own Boys function is external to
 it).  Its outputs are committed; the tests only read the .npz files.
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference tree>
+
+(or with VLX_REFERENCE_DIR=<reference tree> in the environment)
 
 Writes:
   eri_components.npz  every one of the 81 s/p/d classes, bare component
@@ -513,9 +515,12 @@ def build_tiny(classes, rng):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("VLX_REFERENCE_DIR"),
+                    help="the vlx-twoe-ints source tree (default: $VLX_REFERENCE_DIR)")
     ap.add_argument("--only", choices=["components", "tiny", "grad", "f"], default=None)
     args = ap.parse_args()
+    if not args.ref or not os.path.isdir(args.ref):
+        ap.error("the reference tree is needed: --ref <dir> or VLX_REFERENCE_DIR")
     classes = Classes(args.ref)
     if args.only in (None, "components"):
         comp = make_components(classes, np.random.default_rng(1234))

@@ -141,32 +141,30 @@ def test_range_separated_exchange_vs_oracle():
         assert close(matK[k].cpu().numpy(), oK[k]), k
 
 
-def test_small_sp_workload_sampled_rows():
-    """The 5-atom 3s+2p workload (45 Cartesian AOs): 48 random rows of every
-    class against the oracle."""
+def test_small_sp_workload_full_vs_oracle():
+    """The 5-atom 3s+2p workload (45 Cartesian AOs) in full: every entry of
+    every J and K list, the AO J and K and the energy against the FP64 oracle,
+    at an absolute bar of 1e-10 (the FP64 bar) besides the relative one."""
     lib().init(0)
     wl = basis.config_small(0)
     rl = lists.build_lists(wl.mol, wl.D, wl.threshold, fock.gpu_schwarz_fn())
     dl = fock.to_device(rl)
     matJ, matK = fock.build_jk(dl)
     torch.cuda.synchronize()
-    rng = np.random.default_rng(0)
-    for ab in rl.jlists:
-        n = len(rl.jlists[ab].first)
-        rows = np.sort(rng.choice(n, size=min(48, n), replace=False))
-        exp = np.zeros(n)
-        for cd in rl.jlists:
-            if lists.LV[cd[0]] <= lists.LV[cd[1]]:
-                exp += helpers.oracle_J(rl, ab + cd, rows=rows)
-        assert close(matJ[ab].cpu().numpy()[rows], exp[rows]), ab
-    for ac in rl.kpairs:
-        n = len(rl.kpairs[ac].pair_i)
-        rows = np.sort(rng.choice(n, size=min(48, n), replace=False))
-        exp = np.zeros(n)
-        for b in "sp":
-            for d in "sp":
-                exp += helpers.oracle_K(rl, ac[0] + b + ac[1] + d, rows=rows)
-        assert close(matK[ac].cpu().numpy()[rows], exp[rows]), ac
+    oJ, oK = helpers.oracle_jk_all(rl)
+    gJ = {k: v.cpu().numpy() for k, v in matJ.items()}
+    gK = {k: v.cpu().numpy() for k, v in matK.items()}
+    for k in oJ:
+        assert close(gJ[k], oJ[k]), k
+        assert float(np.abs(gJ[k] - oJ[k]).max()) <= 1e-10, k
+    for k in oK:
+        assert close(gK[k], oK[k]), k
+        assert float(np.abs(gK[k] - oK[k]).max()) <= 1e-10, k
+    J, K = lists.contract_J(rl, gJ), lists.contract_K(rl, gK)
+    Jo, Ko = lists.contract_J(rl, oJ), lists.contract_K(rl, oK)
+    assert np.abs(J - Jo).max() <= 1e-10
+    assert np.abs(K - Ko).max() <= 1e-10
+    assert abs(lists.energy(wl.D, J, K) - lists.energy(wl.D, Jo, Ko)) <= 1e-10
 
 
 def test_bitwise_reproducible():
@@ -327,6 +325,40 @@ def test_mixed_precision_errors_within_tolerance():
         L.set_fp32_cut(0.0)
     J2 = lists.contract_J(rl, {k: v.cpu().numpy() for k, v in mJ.items()})
     assert np.abs(J2 - Jo).max() <= 1e-4 * np.abs(Jo).max()
+
+
+def test_fp32_budget_bounds_the_fp32_work():
+    """The FP32 error budget on top of the cutoff: with every quartet below the
+    cutoff, a vanishing budget leaves no quartet with a non-zero bound in FP32
+    (the FP64 build, bit for bit), an unlimited one runs the whole tail in
+    FP32 (different from FP64, still close), and every kernel variant of the
+    classes honours it."""
+    L = lib()
+    L.init(0)
+    wl, rl = small_system({0: 2, 1: 1, 2: 1}, 3, 4.0, seed=29)
+    dl = fock.to_device(rl)
+    L.set_fp32_cut(0.0)
+    rJ, rK = fock.build_jk(dl)
+    torch.cuda.synchronize()
+    ref = ({k: v.cpu().numpy() for k, v in rJ.items()}, {k: v.cpu().numpy() for k, v in rK.items()})
+    saved = L.get_fp32_budget()
+    out = {}
+    try:
+        L.set_fp32_cut(1e30)
+        for b in (1e-300, 0.0):  # 0 = no budget: the cutoff alone decides
+            L.set_fp32_budget(b)
+            mJ, mK = fock.build_jk(dl)
+            torch.cuda.synchronize()
+            out[b] = ({k: v.cpu().numpy() for k, v in mJ.items()}, {k: v.cpu().numpy() for k, v in mK.items()})
+    finally:
+        L.set_fp32_cut(0.0)
+        L.set_fp32_budget(saved)
+    for t in (0, 1):
+        for k in ref[t]:
+            assert np.array_equal(out[1e-300][t][k], ref[t][k]), (t, k)
+    diff = max(float(np.abs(out[0.0][t][k] - ref[t][k]).max()) for t in (0, 1) for k in ref[t])
+    scale = max(float(np.abs(ref[t][k]).max()) for t in (0, 1) for k in ref[t])
+    assert 0.0 < diff <= 1e-4 * scale
 
 
 @pytest.mark.parametrize("variant", [1, 2, 3, 4])

@@ -5,8 +5,10 @@ memory belongs to their own allocator, plugins that may not allocate): it
 keeps its scratch in a fixed 64 MiB device array of the library.  This file
 is collected last on purpose.  It checks, through the C ABI, that two calls in
 a row give the regular entry point's mat_J within the tolerance of the other
-parity tests, and that a call needing more scratch than the array holds is
-refused before any work is queued.
+parity tests, that warm calls leave the device's free memory and the
+stream-ordered pool's usage untouched (nothing is allocated), and that a call
+needing more scratch than the array holds is refused before any work is
+queued.
 """
 import ctypes
 
@@ -30,6 +32,29 @@ def _noalloc_fn(L):
                   for p in ABI.j_params("ssss")]
     f.restype = ctypes.c_int
     return f
+
+
+def _pool_used_high_reset():
+    """Resets the high watermark of the device's stream-ordered pool (the pool
+    the regular entry points allocate their scratch from) and returns a reader
+    of (used now, high since the reset); None without cuda-python."""
+    try:
+        from cuda.bindings import driver as dr
+        from cuda.bindings import runtime as rt
+    except ImportError:
+        return None
+    err, pool = rt.cudaDeviceGetMemPool(torch.cuda.current_device())
+    if err != rt.cudaError_t.cudaSuccess:
+        return None
+    A = rt.cudaMemPoolAttr
+    rt.cudaMemPoolSetAttribute(pool, A.cudaMemPoolAttrUsedMemHigh, dr.cuuint64_t(0))
+
+    def read():
+        _, used = rt.cudaMemPoolGetAttribute(pool, A.cudaMemPoolAttrUsedMemCurrent)
+        _, high = rt.cudaMemPoolGetAttribute(pool, A.cudaMemPoolAttrUsedMemHigh)
+        return int(used), int(high)
+
+    return read
 
 
 def test_noalloc_matches_regular_entry_point_twice():
@@ -58,6 +83,24 @@ def test_noalloc_matches_regular_entry_point_twice():
     for out in outs:
         got = out.cpu().numpy()
         assert float(np.abs(got - exp).max()) <= RTOL * scale + 1e-14
+
+    # warm calls allocate nothing: the device's free memory and the pool's
+    # usage (high watermark included) stay where they were
+    warm = torch.zeros(n, dtype=torch.float64, device="cuda")
+    A = fock.coulomb_args(dl, "ssss", warm, s)
+    args = [A[p] for p in L.j_params["ssss"]]
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    pool = _pool_used_high_reset()
+    used0 = pool()[0] if pool else None
+    for _ in range(2):
+        assert f(*args) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    if pool:
+        used1, high1 = pool()
+        assert used1 == used0 and high1 <= used0, (used0, used1, high1)
 
 
 def test_noalloc_rejects_oversized_call():

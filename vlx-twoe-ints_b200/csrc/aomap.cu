@@ -145,8 +145,12 @@ extern "C" int vlxb_pairGradientToAtoms(const double* pair_grad, uint64_t grad_s
     using namespace vlxb;
     if (n_atoms <= 0 || !grad_atoms || !rowptr) return VLXB_EINVAL;
     if (grad_stride > (uint64_t)INT64_MAX / 8 || (int64_t)n_atoms * 3 > (int64_t)INT32_MAX) return VLXB_EINVAL;
-    if (grad_stride > 0 && (!pair_grad || !src)) return VLXB_EINVAL;
     cudaStream_t st = (cudaStream_t)stream;
+    if (grad_stride == 0) {  // empty CSR: no pair derivatives to fold
+        VLXB_CHECK_CUDA(cudaMemsetAsync(grad_atoms, 0, sizeof(double) * 3 * (size_t)n_atoms, st));
+        return VLXB_OK;
+    }
+    if (!pair_grad || !src) return VLXB_EINVAL;
     pair_grad_atoms_kernel<<<3 * n_atoms, GA_THREADS, 0, st>>>(pair_grad, (int64_t)grad_stride, weight, rowptr,
                                                                src, grad_atoms);
     note_launches();

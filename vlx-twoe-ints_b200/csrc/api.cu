@@ -45,6 +45,10 @@ int vlxb_setFp32Cutoff(double cutoff) { return vlxb::fp32_cut_set(cutoff); }
 
 double vlxb_getFp32Cutoff(void) { return vlxb::fp32_cut_get(); }
 
+int vlxb_setFp32Budget(double budget) { return vlxb::fp32_budget_set(budget); }
+
+double vlxb_getFp32Budget(void) { return vlxb::fp32_budget_get(); }
+
 const char* vlxb_status_string(int status)
 {
     switch (status) {

@@ -94,6 +94,11 @@ int run_coulomb_impl(const CoulombArgs& a, cudaStream_t st, Arena& ar, const Boy
     rc = jket_prepare<LC, LD>(ar, gk, a.cd_first, a.cd_second, a.cd_D, a.cd_Q, a.cd_pdata, kd,
                               batched ? a.prim_mol_c : nullptr, batched ? a.n_mol : 0, jvar == 2);
     if (rc) return rc;
+    const double budget = (cut > 0.0 && !G) ? fp32_budget_get() : 0.0;
+    if (budget > 0.0) {
+        rc = budget_prefix_kets(ar, kd, LD);
+        if (rc) return rc;
+    }
     int32_t* bmol = nullptr;
     if (batched) {
         rc = bra_record_mol(ar, gb, a.prim_mol_a, &bmol);
@@ -103,7 +108,7 @@ int run_coulomb_impl(const CoulombArgs& a, cudaStream_t st, Arena& ar, const Boy
     if (ar.measuring()) return VLXB_OK;
     JBraRecs bra{gb.rec_sp, gb.rec_q, gb.rec_mask, gb.n_rec, gb.geo, gb.entry, gb.sp_stride, a.ab_pdata, bmol};
     JKetPairs ket{kd.geo, kd.tmax, kd.tmin, kd.Dpp, kd.Dm, kd.Qc, kd.Dc, kd.stride, kd.n, batched ? kd.seg : nullptr,
-                  kd.Dh};
+                  kd.Dh, kd.tpre};
     int grid = launch_grid_limit();
     if ((int64_t)grid > (int64_t)a.n_ab) grid = (int)a.n_ab;
     for (int pm = 0; pm < (cut > 0.0 ? 2 : 1); pm++) {
@@ -118,22 +123,24 @@ int run_coulomb_impl(const CoulombArgs& a, cudaStream_t st, Arena& ar, const Boy
         } else if (jvar == 2) {
             if (pm == 0)
                 coulomb_md_kernel<LA, LB, LC, LD, 0><<<grid, MD_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc,
-                                                                                  cut, 0);
+                                                                                  cut, budget);
             else
                 coulomb_md_kernel<LA, LB, LC, LD, 1><<<grid, MD_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc,
-                                                                                  cut, 0);
+                                                                                  cut, budget);
         } else if (jvar == 1) {
             if (pm == 0)
                 coulomb_col_kernel<LA, LB, LC, LD, 0><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc,
-                                                                                  cut);
+                                                                                  cut, budget);
             else
                 coulomb_col_kernel<LA, LB, LC, LD, 1><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc,
-                                                                                  cut);
+                                                                                  cut, budget);
         } else {
             if (pm == 0)
-                coulomb_kernel<LA, LB, LC, LD, 0><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut);
+                coulomb_kernel<LA, LB, LC, LD, 0><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut,
+                                                                               budget);
             else
-                coulomb_kernel<LA, LB, LC, LD, 1><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut);
+                coulomb_kernel<LA, LB, LC, LD, 1><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc, cut,
+                                                                               budget);
         }
         note_launches();
     }
@@ -212,6 +219,7 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
         if (rc) return rc;
     }
     const int var = schedule_get(1, LA, LB, LC, LD);
+    const double budget = cut > 0.0 ? fp32_budget_get() : 0.0;
     KGroups kgab{}, kgcd{};
     const uint32_t key_naos = a.key_naos ? a.key_naos : a.naos;
     if (var == 3 || var == 4) {
@@ -224,8 +232,21 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
             rc = contract_groups(ar, npc, gcd, a.aoinds[LD], key_naos);
             if (rc) return rc;
         }
-        kgab = KGroups{gab.gseg, gab.gq, gab.gbeg, gab.gcnt, gab.msp, gab.mq, gab.msu, gab.mmask};
-        kgcd = KGroups{gcd.gseg, gcd.gq, gcd.gbeg, gcd.gcnt, gcd.msp, gcd.mq, gcd.msu, gcd.mmask};
+    }
+    if (budget > 0.0) {
+        // after contract_groups: groups get their amplified sums too
+        rc = budget_prefix_records(ar, gab, npa, LB);
+        if (rc) return rc;
+        if (same) {
+            gcd = gab;
+        } else {
+            rc = budget_prefix_records(ar, gcd, npc, LD);
+            if (rc) return rc;
+        }
+    }
+    if (var == 3 || var == 4) {
+        kgab = KGroups{gab.gseg, gab.gq, gab.gbeg, gab.gcnt, gab.msp, gab.mq, gab.msu, gab.mmask, gab.gqa, gab.gqpre};
+        kgcd = KGroups{gcd.gseg, gcd.gq, gcd.gbeg, gcd.gcnt, gcd.msp, gcd.mq, gcd.msu, gcd.mmask, gcd.gqa, gcd.gqpre};
     }
     double* blk_maxD = nullptr;
     if (a.prim_mol_a && a.maxD_mol) {
@@ -233,8 +254,10 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
         if (rc) return rc;
     }
     KOutBlocks out{ko.ish, ko.ksh, ko.idx, ko.stride, ko.n, blk_maxD};
-    KPartnerRecs rab{gab.rec_sp, gab.rec_q, gab.rec_mask, gab.seg, gab.geo, gab.S, gab.sp_j, gab.sp_stride, gab.su};
-    KPartnerRecs rcd{gcd.rec_sp, gcd.rec_q, gcd.rec_mask, gcd.seg, gcd.geo, gcd.S, gcd.sp_j, gcd.sp_stride, gcd.su};
+    KPartnerRecs rab{gab.rec_sp, gab.rec_q, gab.rec_mask, gab.seg, gab.geo, gab.S, gab.sp_j, gab.sp_stride, gab.su,
+                     gab.rec_qa, gab.rec_qpre};
+    KPartnerRecs rcd{gcd.rec_sp, gcd.rec_q, gcd.rec_mask, gcd.seg, gcd.geo, gcd.S, gcd.sp_j, gcd.sp_stride, gcd.su,
+                     gcd.rec_qa, gcd.rec_qpre};
     int grid = launch_grid_limit();
     if ((int64_t)grid > (int64_t)a.n_ik) grid = (int)a.n_ik;
     unsigned long long* qc = quartet_counters_device();
@@ -247,10 +270,10 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
             if (var == 3) {
                 if (pm == 0)
                     exchange_colc_kernel<LA, LB, LC, LD, 0, 0><<<grid, K_THREADS, 0, st>>>(
-                        out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut);
+                        out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
                 else
                     exchange_colc_kernel<LA, LB, LC, LD, 0, 1><<<grid, K_THREADS, 0, st>>>(
-                        out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut);
+                        out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
                 launched = true;
             }
         }
@@ -258,10 +281,10 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
             if (var == 4) {
                 if (pm == 0)
                     exchange_colc_kernel<LA, LB, LC, LD, 1, 0><<<grid, K_THREADS, 0, st>>>(
-                        out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut);
+                        out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
                 else
                     exchange_colc_kernel<LA, LB, LC, LD, 1, 1><<<grid, K_THREADS, 0, st>>>(
-                        out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut);
+                        out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
                 launched = true;
             }
         }
@@ -269,10 +292,10 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
             if (var == 1) {
                 if (pm == 0)
                     exchange_col_kernel<LA, LB, LC, LD, 0, 0><<<grid, K_THREADS, 0, st>>>(
-                        out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut);
+                        out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
                 else
                     exchange_col_kernel<LA, LB, LC, LD, 0, 1><<<grid, K_THREADS, 0, st>>>(
-                        out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut);
+                        out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
                 launched = true;
             }
         }
@@ -280,20 +303,20 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
             if (var == 2) {
                 if (pm == 0)
                     exchange_col_kernel<LA, LB, LC, LD, 1, 0><<<grid, K_THREADS, 0, st>>>(
-                        out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut);
+                        out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
                 else
                     exchange_col_kernel<LA, LB, LC, LD, 1, 1><<<grid, K_THREADS, 0, st>>>(
-                        out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut);
+                        out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
                 launched = true;
             }
         }
         if (!launched) {
             if (pm == 0)
                 exchange_kernel<LA, LB, LC, LD, 0><<<grid, K_THREADS, 0, st>>>(out, rab, rcd, dm, a.maxD, a.omega,
-                                                                               a.thr, a.mat_K, tab, qk, cut);
+                                                                               a.thr, a.mat_K, tab, qk, cut, budget);
             else
                 exchange_kernel<LA, LB, LC, LD, 1><<<grid, K_THREADS, 0, st>>>(out, rab, rcd, dm, a.maxD, a.omega,
-                                                                               a.thr, a.mat_K, tab, qk, cut);
+                                                                               a.thr, a.mat_K, tab, qk, cut, budget);
         }
         note_launches();
     }
@@ -350,8 +373,10 @@ int run_exchange_grad(const ExchangeArgs& a, int64_t gstride, cudaStream_t st)
     }
     if (ar.failed()) return VLXB_ENOMEM;
     KOutBlocks out{ko.ish, ko.ksh, ko.idx, ko.stride, ko.n, nullptr};
-    KPartnerRecs rab{gab.rec_sp, gab.rec_q, gab.rec_mask, gab.seg, gab.geo, gab.S, gab.sp_j, gab.sp_stride, gab.su};
-    KPartnerRecs rcd{gcd.rec_sp, gcd.rec_q, gcd.rec_mask, gcd.seg, gcd.geo, gcd.S, gcd.sp_j, gcd.sp_stride, gcd.su};
+    KPartnerRecs rab{gab.rec_sp, gab.rec_q, gab.rec_mask, gab.seg, gab.geo, gab.S, gab.sp_j, gab.sp_stride, gab.su,
+                     nullptr, nullptr};
+    KPartnerRecs rcd{gcd.rec_sp, gcd.rec_q, gcd.rec_mask, gcd.seg, gcd.geo, gcd.S, gcd.sp_j, gcd.sp_stride, gcd.su,
+                     nullptr, nullptr};
     const KDensity dm{a.aoinds[LB], a.count[LB], a.aoinds[LD], a.count[LD], a.D, a.naos};
     const KGradBlockD bd{a.aoinds[LA], a.count[LA], a.aoinds[LC], a.count[LC], LA == LC ? 1 : 0};
     int grid = launch_grid_limit();

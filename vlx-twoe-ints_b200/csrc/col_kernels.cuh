@@ -199,7 +199,7 @@ template <int LA, int LB, int LC, int LD, int ORI, int PM>
 __global__ void __launch_bounds__(K_THREADS)
 exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity dm, double maxD, double omega,
                     double thr, double* __restrict__ mat_K, BoysTabs tabs, unsigned long long* __restrict__ qcount,
-                    double fp32_cut)
+                    double fp32_cut, double fp32_budget)
 {
     using S = KColShape<LA, LB, LC, LD, ORI>;
     constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND;
@@ -232,7 +232,7 @@ exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity d
 
         for (int jb = a0; jb < a1; jb += K_JCHUNK) {
             const int nj = min(K_JCHUNK, a1 - jb);
-            k_chunk_scan(ab, cd, jb, nj, c0, c1, mD, thr, fp32_cut, ch);
+            k_chunk_scan(ab, cd, jb, nj, c0, c1, mD, thr, fp32_cut, ch, a1 - a0, fp32_budget);
             const int t64 = s_c64[nj], t32 = s_c32[nj];
             if (qcount && PM == 0 && threadIdx.x == 0) atomicAdd(qcount, (unsigned long long)(t64 + t32));
             const int n64 = PM == 0 ? (t64 + NW * P - 1) / (NW * P) : 0;
@@ -309,6 +309,8 @@ struct KGroups {
     const double* mq;        // member q
     const double* msu;       // member uniform S, or NaN (member alone in its group)
     const uint64_t* mmask;   // member component mask
+    const double* qa;        // sum over members of |q| times HRR growth (FP32 error budget), or null
+    const double* qpre;      // inclusive prefix sum of qa, or null
 };
 
 template <int LA, int LB, int LC, int LD, int ORI, typename T>
@@ -446,7 +448,7 @@ template <int LA, int LB, int LC, int LD, int ORI, int PM>
 __global__ void __launch_bounds__(K_THREADS, 3)
 exchange_colc_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KGroups gab, KGroups gcd, KDensity dm,
                      double maxD, double omega, double thr, double* __restrict__ mat_K, BoysTabs tabs,
-                     unsigned long long* __restrict__ qcount, double fp32_cut)
+                     unsigned long long* __restrict__ qcount, double fp32_cut, double fp32_budget)
 {
     using S = KColShape<LA, LB, LC, LD, ORI>;
     constexpr int NA = S::NA, NB = S::NB, NC = S::NC, ND = S::ND;
@@ -480,7 +482,8 @@ exchange_colc_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KGroups g
 
         for (int jb = a0; jb < a1; jb += K_JCHUNK) {
             const int nj = min(K_JCHUNK, a1 - jb);
-            k_chunk_scan(gab.q, gcd.q, jb, nj, c0, c1, mD, thr, fp32_cut, ch);
+            k_chunk_scan(gab.q, gcd.q, jb, nj, c0, c1, mD, thr, fp32_cut, ch, gab.qa, gcd.qpre, a1 - a0,
+                         fp32_budget);
             const int t64 = s_c64[nj], t32 = s_c32[nj];
             const int n64 = PM == 0 ? (t64 + NW * P - 1) / (NW * P) : 0;
             for (int it = 0; it < n64; it++) {
@@ -562,7 +565,7 @@ __device__ __forceinline__ void jcol_quartet(bool act, const PairGeo& b, double 
 template <int LA, int LB, int LC, int LD, int PM>
 __global__ void __launch_bounds__(J_THREADS)
 coulomb_col_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double thr, BoysTabs tabs,
-                   unsigned long long* __restrict__ qcount, double fp32_cut)
+                   unsigned long long* __restrict__ qcount, double fp32_cut, double fp32_budget)
 {
     using CT = ColTab<LA, LB, LC, LD, 0>;
     constexpr int NE = nrange(LA, LB), NF = nrange(LC, LD);
@@ -591,7 +594,7 @@ coulomb_col_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, doub
         }
         if (threadIdx.x == 0) {
             int ncut, nexact, n64;
-            ket_prefixes(ket, k0, k1, qb, thr, fp32_cut, ncut, nexact, n64);
+            ket_prefixes(ket, k0, k1, qb, thr, fp32_cut, fabs(qb) * pair_amp(b, LB), fp32_budget, ncut, nexact, n64);
             s_ncut = ncut;
             s_n64 = n64;
             if (qcount && PM == 0) atomicAdd(qcount, (unsigned long long)(nexact - k0));

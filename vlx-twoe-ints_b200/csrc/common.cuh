@@ -63,36 +63,34 @@ __device__ __forceinline__ void boys_f64(double T, const double* __restrict__ ta
     }
 }
 
-// FP32 variant for the mixed-precision path: the Boys argument T arrives in
-// FP64; F_L from a float copy of the same table (4 Taylor terms: truncation
-// < 2e-8 relative, below float rounding), recursions in float.
-constexpr int BOYS_NT32 = 4;
-
+// FP32 variant for the mixed-precision path.  F_L and e^-T come from the FP64
+// evaluation above (the same table, 8 Taylor terms, FP64 exp), rounded once
+// to float, so the Boys values carry no error beyond one float rounding; only
+// the short recursion runs in float.  This costs a few FP64 operations per
+// quartet and removes the bias a float table and a fast exponential put into
+// every FP32 quartet.
 template <int L>
-__device__ __forceinline__ void boys_f32(double Td, const float* __restrict__ tab, float* F)
+__device__ __forceinline__ void boys_f32(double Td, const double* __restrict__ tab, float* F)
 {
     if (Td < BOYS_TMAX) {
         const int k = __double2int_rn(Td * BOYS_INV_H);
-        const float md = (float)((double)k * BOYS_H - Td);
-        const float T = (float)Td;
-        const float* row = tab + k * BOYS_NCOL + L;
-        float acc = __ldg(row + BOYS_NT32 - 1);
+        const double md = (double)k * BOYS_H - Td;
+        const double* row = tab + k * BOYS_NCOL + L;
+        double acc = __ldg(row + BOYS_NT - 1);
 #pragma unroll
-        for (int j = BOYS_NT32 - 1; j >= 1; j--) acc = fmaf(acc, md * (1.0f / j), __ldg(row + j - 1));
-        F[L] = acc;
+        for (int j = BOYS_NT - 1; j >= 1; j--) acc = fma(acc, md * (1.0 / j), __ldg(row + j - 1));
+        F[L] = (float)acc;
         if (L > 0) {
-            const float ex = __expf(-T);
-            const float t2 = 2.0f * T;
+            const float ex = (float)exp(-Td);
+            const float t2 = (float)(2.0 * Td);
 #pragma unroll
             for (int m = L - 1; m >= 0; m--) F[m] = fmaf(t2, F[m + 1], ex) * (1.0f / (2.0f * m + 1.0f));
         }
     } else {
-        const float T = (float)Td;
-        const float inv_t = 1.0f / T;
-        F[0] = (float)SQRT_PI_4 * sqrtf(inv_t);
+        F[0] = (float)(SQRT_PI_4 * sqrt(1.0 / Td));
         if (L > 0) {
-            const float ex = __expf(-T);
-            const float h = 0.5f * inv_t;
+            const float ex = (float)exp(-Td);
+            const float h = (float)(0.5 / Td);
 #pragma unroll
             for (int m = 0; m < L; m++) F[m + 1] = fmaf((2.0f * m + 1.0f), F[m], -ex) * h;
         }
@@ -171,10 +169,10 @@ __device__ __forceinline__ void make_quartet(const PairGeo& b, const PairGeo& k,
 }
 
 // Mixed-precision variant of make_quartet: every quartet scalar and the Boys
-// argument are formed in FP64 and rounded to float; F_m in float.
+// argument are formed in FP64 and rounded to float; F_m in float (boys_f32).
 template <int L>
 __device__ __forceinline__ void make_quartet_f32(const PairGeo& b, const PairGeo& k, double omega,
-                                                 const float* __restrict__ boys_tab32, QVT<float>& q, float* F)
+                                                 const double* __restrict__ boys_tab, QVT<float>& q, float* F)
 {
     const double inv = 1.0 / (b.z + k.z);
     const double rho = b.z * k.z * inv;
@@ -192,7 +190,7 @@ __device__ __forceinline__ void make_quartet_f32(const PairGeo& b, const PairGeo
     double d2 = 1.0;
     if (omega != 0.0) d2 = omega * omega / (rho + omega * omega);
     const double rd = rho * d2;
-    boys_f32<L>(rd * r2, boys_tab32, F);
+    boys_f32<L>(rd * r2, boys_tab, F);
     const float lam = (float)(2.0 * sqrt(rd * INV_PI_D));
     float s = lam;
     const float d2f = (float)d2;
@@ -213,7 +211,7 @@ __device__ __forceinline__ void make_quartet_t(const PairGeo& b, const PairGeo& 
                                                const double* __restrict__ tab64, const float* __restrict__ tab32,
                                                QVT<float>& q, float* F)
 {
-    make_quartet_f32<L>(b, k, omega, tab32, q, F);
+    make_quartet_f32<L>(b, k, omega, tab64, q, F);
 }
 
 template <int LA, int LB, int LC, int LD, typename T>

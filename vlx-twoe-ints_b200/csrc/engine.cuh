@@ -106,6 +106,12 @@ const float* boys_table32_device();
 // (0 = plain FP64, the default of the drop-in entry points).
 double fp32_cut_get();
 int fp32_cut_set(double cut);
+// FP32 error budget (0 = none, the cutoff alone decides): among the quartets
+// below the cutoff, only the tail of each bra's ket list (J) or of each
+// (i, k) block's partner list per j (K) whose summed error proxy (bounds
+// times hrr_amp on both pairs) stays within the budget runs in FP32.
+double fp32_budget_get();
+int fp32_budget_set(double budget);
 
 // Per-device counters of screened-in primitive shell quartets processed by
 // the J ([0]) and K ([1]) kernels (device memory, allocated with the table).
@@ -142,6 +148,12 @@ struct PairGroups {
     double* mq = nullptr;      // [rec_stride] member q
     double* msu = nullptr;     // [rec_stride] member uniform S or NaN (then alone in its group)
     uint64_t* mmask = nullptr; // [rec_stride] member component mask
+    // FP32 error budget (budget_prefix_records; null when no budget is set):
+    // per record / group the amplified bound, and its inclusive prefix sum
+    double* rec_qa = nullptr;
+    double* rec_qpre = nullptr;
+    double* gqa = nullptr;
+    double* gqpre = nullptr;
 };
 
 // Largest number of partner records summed before one HRR.
@@ -160,6 +172,12 @@ int make_records(Arena& ar, int nxy, PairGroups& g, const double* Q, int64_t n_e
 // Sort records by descending q inside segments of the first primitive shell,
 // and fill per-shell-pair S from the caller's pair data.
 int segment_records(Arena& ar, int nxy, int npa, int npb, PairGroups& g, const double* pdata);
+// Amplified bounds and their prefix sums for the FP32 budget (records, and
+// groups when contract_groups ran); lh = angular momentum the pair's HRR moves.
+int budget_prefix_records(Arena& ar, PairGroups& g, int npa, int lh);
+// The same for the sorted J kets (tpre), lh = the ket's second angular momentum.
+struct JKetData;
+int budget_prefix_kets(Arena& ar, JKetData& kd, int lh);
 // Group segmented partner records by the partner's contracted shell (same AO
 // indices, part_aoinds = the partner type's prim_aoinds) for the contracted
 // exchange kernels.
@@ -171,6 +189,7 @@ struct JKetData {
     int* n;
     int* seg = nullptr;  // [n_mol + 1] ket offsets per molecule (batched calls)
     double* Dh = nullptr;  // [stride][nherm(LC + LD)] Hermite ket density (McMurchie-Davidson kernel)
+    double* tpre = nullptr;  // inclusive prefix sum of tmax * hrr_amp over the sorted kets (FP32 budget)
 };
 // prim_mol_c (batched calls, else null): molecule of every type-c primitive;
 // the kets are then sorted by molecule, and by descending bound inside one.

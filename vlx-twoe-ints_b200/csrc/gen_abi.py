@@ -170,11 +170,24 @@ def header():
          "int vlxb_getSchedule(int kind, int la, int lb, int lc, int ld);", "",
          "/* Mixed precision: shell quartets whose screening bound (|Q_ij| max|Q_kl D_kl|",
          "   for J, |Q_ij Q_kl max_D| for K) is below `cutoff` are evaluated in FP32",
-         "   (Boys argument in FP64), everything else and all accumulation in FP64.",
-         "   0 (the default) = plain FP64, the drop-in behaviour.  Process-wide.",
-         "   No reference counterpart. */",
+         "   (Boys argument and Boys values in FP64, rounded once), everything else",
+         "   and all accumulation in FP64.  0 (the default) = plain FP64, the drop-in",
+         "   behaviour.  Process-wide.  No reference counterpart. */",
          "int vlxb_setFp32Cutoff(double cutoff);",
          "double vlxb_getFp32Cutoff(void);", "",
+         "/* FP32 error budget (with a cutoff > 0; default 1e-3; 0 = no budget, the",
+         "   cutoff alone decides).  A quartet below the cutoff runs in FP32 only inside the tail",
+         "   of its list whose summed error proxy stays within `budget`: per J bra",
+         "   record, |Q_ij| A_ij * sum over the FP32 kets of max|Q_kl D_kl| A_kl; per",
+         "   K output block and partner j, |Q_ij| A_ij max_D * sum over the FP32 l",
+         "   of |Q_kl| A_kl, against budget / (the block's number of j).  A is the",
+         "   growth the horizontal recurrence gives rounding errors across a pair,",
+         "   (1 + sqrt(2 zeta) |R|)^l (R = AB or CD, l the momentum it moves).  The",
+         "   FP32 error of an output element then scales with the budget, not with",
+         "   the number of quartets below the cutoff.  Process-wide.  No reference",
+         "   counterpart. */",
+         "int vlxb_setFp32Budget(double budget);",
+         "double vlxb_getFp32Budget(void);", "",
          "/* Primitive-pair -> AO contraction (the step after the class entry points,",
          "   whose mat_J / mat_K hold one value per list entry, gen_coulomb.py:296,",
          "   gen_exchange.py:341; the reference's caller does it on the host).",
@@ -260,7 +273,8 @@ def header():
          "   return VLXB_ETOOBIG before queuing any work.  The first call on a device",
          "   resolves the array and uploads the Boys tables (synchronously): make it",
          "   before any stream capture.  Calls share the array, so calls that overlap",
-         "   on the GPU race; serialise them. */",
+         "   on the GPU race; serialise them.  Its quartets are not added to the",
+         "   counters of vlxb_quartetCounters (those live in allocated memory). */",
          "#define VLXB_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)",
          "int vlxb_computeCoulombFockSSSS_noalloc(" + ", ".join(j_params("ssss")) + ");", ""]
     L.append("/* ---- Coulomb: replace computeCoulombFock<ABCD> of gen_coulomb.py:74-93 ---- */")
@@ -292,8 +306,10 @@ def header():
           "   p = src[e] & 0x7fffffff (< grad_stride) and side = src[e] >> 31 (0:",
           "   first centre, 1: second); weight NULL = 1 (the exchange gradient comes",
           "   weighted).  Overwrites grad_atoms (3 * n_atoms doubles).  Entries are",
-          "   summed in a fixed order: results are bit-reproducible.  No reference",
-          "   counterpart. */",
+          "   summed in a fixed order: results are bit-reproducible.  grad_stride 0",
+          "   means an empty CSR (no pair derivatives): grad_atoms is zeroed and",
+          "   nothing else is read; otherwise pair_grad and src must be non-NULL.",
+          "   No reference counterpart. */",
           "int vlxb_pairGradientToAtoms(const double* pair_grad, uint64_t grad_stride, const double* weight,",
           "                             const int64_t* rowptr, const uint32_t* src, int32_t n_atoms,",
           "                             double* grad_atoms, void* stream);",
@@ -308,7 +324,10 @@ def header():
           "       w_ik D_ik sum_jl D_jl d(ij|kl)/dX_x,",
           "   X = (A_x, A_y, A_z, C_x, C_y, C_z) the centres of i and k, D the AO",
           "   density (D_ik = mat_D_full_AO[ao(i)][ao(k)]), w_ik = 1 for i == k of a",
-          "   same-type list, else 2; the block's other positions receive nothing.",
+          "   same-type list, else 2; the block's other positions receive nothing,",
+          "   so grad_K is meaningful per primitive shell block only (unlike the",
+          "   Coulomb gradient's per-entry values): fold it onto atoms with",
+          "   vlxb_pairGradientToAtoms (weight NULL), never read it per entry.",
           "   Summed over the 54 classes and credited to the atoms of i (x < 3) and",
           "   k (x >= 3) this is dE_K/dR for E_K = 1/2 Tr[D K] (the j and l centres",
           "   are covered by the symmetry of the sum).  Same screening and omega as",

@@ -1,7 +1,7 @@
 // Coulomb nuclear-gradient kernel: bra-centre derivatives of J in
 // McMurchie-Davidson form, with several quartets per warp.
 //
-// Same mathematics as coulomb_md_kernel<..., G = 1> (md_kernels.cuh): the
+// Same mathematics as coulomb_md_kernel (md_kernels.cuh) one derivative up: the
 // bra Hermite range grows by one level (R up to L + 1, X_e up to
 // LA + LB + 1) and the epilogue sums E^{a+-1,b} and E^{a,b+-1} against X:
 //   dJ_ab/dA_x = S_ab sum_e (2 alpha E^{a+1x,b}_e - a_x E^{a-1x,b}_e) X_e,
@@ -127,7 +127,7 @@ coulomb_grad_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ grad, int6
         }
         if (threadIdx.x == 0) {
             int ncut, nexact, n64;
-            ket_prefixes(ket, k0, k1, qb, thr, fp32_cut, ncut, nexact, n64);
+            ket_prefixes(ket, k0, k1, qb, thr, fp32_cut, 0.0, 0.0, ncut, nexact, n64);
             s_ncut = ncut;
             s_n64 = n64;
         }
@@ -208,7 +208,7 @@ coulomb_grad_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ grad, int6
                     }
                 } else {
                     float F[L + 1];
-                    boys_f32<L>(T2, tabs.f32, F);
+                    boys_f32<L>(T2, tabs.f64, F);
                     float s = (float)(2.0 * sqrt(rho * INV_PI_D));
                     const float m2r = (float)(-2.0 * rho);
 #pragma unroll

@@ -61,6 +61,7 @@ struct JKetPairs {
     const int* n;
     const int* seg;      // [molecules + 1] ket range of each molecule (batched calls), or null
     const double* Dh;    // [stride][nherm(LC+LD)] Hermite ket density (McMurchie-Davidson kernel), or null
+    const double* tpre;  // [stride] inclusive prefix sum of tmax * HRR growth (FP32 error budget), or null
 };
 
 struct BoysTabs {
@@ -116,14 +117,29 @@ __device__ __forceinline__ void j_quartet(const PairGeo& b, double qb, const JKe
     }
 }
 
+// HRR growth factor of a pair (the factor hrr_amp of the list preparation,
+// from the pair's geometry record): (1 + sqrt(2 zeta) |R|)^lh.
+__device__ __forceinline__ double pair_amp(const PairGeo& g, int lh)
+{
+    if (lh == 0) return 1.0;
+    const double f = 1.0 + sqrt(2.0 * g.z * (g.Rx * g.Rx + g.Ry * g.Ry + g.Rz * g.Rz));
+    double a = f;
+    for (int k = 1; k < lh; k++) a *= f;
+    return a;
+}
+
 // Prefix lengths of the descending ket bound list for one bra: ncut (slack
 // included: candidates), nexact (screened-in quartets, for the counters),
-// n64 (bound >= fp32_cut: evaluated in FP64; all of ncut when fp32_cut <= 0).
+// n64 (evaluated in FP64; all of ncut when fp32_cut <= 0).
 // Kets k0 <= t < k1 (one molecule's, sorted by descending bound): ncut / nexact
 // / n64 = end (absolute index) of the kets inside the screening slack band /
-// passing the exact screen / at or above the FP32 cutoff.
+// passing the exact screen / in FP64.  A ket runs in FP32 when its bound is
+// below fp32_cut and, with a budget > 0, when it lies in the tail [n64, ncut)
+// whose summed error proxy qa * sum(tmax * HRR growth) stays <= budget
+// (qa = the bra's Q times its own HRR growth).
 __device__ __forceinline__ void ket_prefixes(const JKetPairs& ket, int k0, int k1, double qb, double thr,
-                                             double fp32_cut, int& ncut, int& nexact, int& n64)
+                                             double fp32_cut, double qa, double budget, int& ncut, int& nexact,
+                                             int& n64)
 {
     int lo = k0, hi = k1;
     while (lo < hi) {
@@ -149,6 +165,17 @@ __device__ __forceinline__ void ket_prefixes(const JKetPairs& ket, int k0, int k
             else hi3 = mid;
         }
         n64 = lo3;
+        if (budget > 0.0 && ket.tpre && n64 < ncut) {
+            const double pend = __ldg(ket.tpre + ncut - 1);
+            int lo4 = n64, hi4 = ncut;
+            while (lo4 < hi4) {
+                const int mid = (lo4 + hi4) >> 1;
+                const double tail = pend - (mid > 0 ? __ldg(ket.tpre + mid - 1) : 0.0);
+                if (qa * tail <= budget) hi4 = mid;
+                else lo4 = mid + 1;
+            }
+            n64 = lo4;
+        }
     }
 }
 
@@ -159,7 +186,7 @@ __device__ __forceinline__ void ket_prefixes(const JKetPairs& ket, int k0, int k
 template <int LA, int LB, int LC, int LD, int PM>
 __global__ void __launch_bounds__(J_THREADS)
 coulomb_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double thr, BoysTabs tabs,
-               unsigned long long* __restrict__ qcount, double fp32_cut)
+               unsigned long long* __restrict__ qcount, double fp32_cut, double fp32_budget)
 {
     constexpr int NE = nrange(LA, LB);
     constexpr int NAB = ncart(LA) * ncart(LB);
@@ -182,7 +209,7 @@ coulomb_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double t
         }
         if (threadIdx.x == 0) {
             int ncut, nexact, n64;
-            ket_prefixes(ket, k0, k1, qb, thr, fp32_cut, ncut, nexact, n64);
+            ket_prefixes(ket, k0, k1, qb, thr, fp32_cut, fabs(qb) * pair_amp(b, LB), fp32_budget, ncut, nexact, n64);
             s_ncut = ncut;
             s_n64 = n64;
             if (qcount && PM == 0) atomicAdd(qcount, (unsigned long long)(nexact - k0));
@@ -254,6 +281,8 @@ struct KPartnerRecs {
     const int32_t* partner;    // [sp_stride] partner primitive shell (j or l)
     int64_t sp_stride;
     const double* su;          // [n_rec] S shared by all components of the record, or NaN
+    const double* qa;          // [n_rec] |q| times the record's HRR growth (FP32 error budget), or null
+    const double* qpre;        // [n_rec] inclusive prefix sum of qa, or null
 };
 
 struct KDensity {
@@ -275,9 +304,14 @@ struct KChunk {
     int* c32;
 };
 
+// FP32 error budget (budget > 0, aqa / cqpre non-null): the l tail of j runs
+// in FP32 only as far as |q_j| A_j max_D * sum(|q_l| A_l) stays within
+// budget / njtot (njtot = the block's j count, A the HRR growth of a pair).
 __device__ __forceinline__ void k_chunk_scan(const double* __restrict__ aq, const double* __restrict__ cq, int jb,
                                              int nj, int c0, int c1, double maxD, double thr, double fp32_cut,
-                                             KChunk s)
+                                             KChunk s, const double* __restrict__ aqa = nullptr,
+                                             const double* __restrict__ cqpre = nullptr, int njtot = 1,
+                                             double budget = 0.0)
 {
     for (int t = threadIdx.x; t < nj; t += blockDim.x) {
         const double qij = __ldg(aq + jb + t);
@@ -297,6 +331,19 @@ __device__ __forceinline__ void k_chunk_scan(const double* __restrict__ aq, cons
                 else hi2 = mid;
             }
             n64 = lo2 - c0;
+            if (budget > 0.0 && aqa && cqpre && n64 < nl) {
+                const double qa = __ldg(aqa + jb + t) * fabs(maxD);
+                const double bj = budget / (double)(njtot > 0 ? njtot : 1);
+                const double pend = __ldg(cqpre + c0 + nl - 1);
+                int lo4 = c0 + n64, hi4 = c0 + nl;
+                while (lo4 < hi4) {
+                    const int mid = (lo4 + hi4) >> 1;
+                    const double tail = pend - (mid > 0 ? __ldg(cqpre + mid - 1) : 0.0);
+                    if (qa * tail <= bj) hi4 = mid;
+                    else lo4 = mid + 1;
+                }
+                n64 = lo4 - c0;
+            }
         }
         s.nl[t] = nl;
         s.n64[t] = n64;
@@ -314,9 +361,10 @@ __device__ __forceinline__ void k_chunk_scan(const double* __restrict__ aq, cons
 }
 
 __device__ __forceinline__ void k_chunk_scan(const KPartnerRecs& ab, const KPartnerRecs& cd, int jb, int nj, int c0,
-                                             int c1, double maxD, double thr, double fp32_cut, KChunk s)
+                                             int c1, double maxD, double thr, double fp32_cut, KChunk s,
+                                             int njtot = 1, double budget = 0.0)
 {
-    k_chunk_scan(ab.rec_q, cd.rec_q, jb, nj, c0, c1, maxD, thr, fp32_cut, s);
+    k_chunk_scan(ab.rec_q, cd.rec_q, jb, nj, c0, c1, maxD, thr, fp32_cut, s, ab.qa, cd.qpre, njtot, budget);
 }
 
 // index t of the last entry with c[t] <= w (c ascending, c[0] = 0 <= w)
@@ -403,7 +451,8 @@ __device__ __forceinline__ void k_quartet(const KPartnerRecs& ab, const KPartner
 template <int LA, int LB, int LC, int LD, int PM>
 __global__ void __launch_bounds__(K_THREADS)
 exchange_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity dm, double maxD, double omega, double thr,
-                double* __restrict__ mat_K, BoysTabs tabs, unsigned long long* __restrict__ qcount, double fp32_cut)
+                double* __restrict__ mat_K, BoysTabs tabs, unsigned long long* __restrict__ qcount, double fp32_cut,
+                double fp32_budget)
 {
     constexpr int NA = ncart(LA), NC = ncart(LC);
     constexpr int NAC = NA * NC;
@@ -425,7 +474,7 @@ exchange_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity dm, d
 
         for (int jb = a0; jb < a1; jb += K_JCHUNK) {
             const int nj = min(K_JCHUNK, a1 - jb);
-            k_chunk_scan(ab, cd, jb, nj, c0, c1, mD, thr, fp32_cut, ch);
+            k_chunk_scan(ab, cd, jb, nj, c0, c1, mD, thr, fp32_cut, ch, a1 - a0, fp32_budget);
             const int t64 = s_c64[nj], t32 = s_c32[nj];
             if (qcount && PM == 0 && threadIdx.x == 0) atomicAdd(qcount, (unsigned long long)(t64 + t32));
             if (PM == 0) {

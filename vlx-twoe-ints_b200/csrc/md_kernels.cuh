@@ -12,19 +12,9 @@
 // J_ab = S_ab sum_e E^{ab}_e X_e per present component pair.  Same screening,
 // same counters, same FP32/FP64 passes as coulomb_kernel; no atomics on J.
 //
-// G = 1 is the nuclear-gradient form of the same kernel: the derivative of
-// each bra list entry's J value with respect to the bra centres, with the
-// ket (density included) held fixed.  A Cartesian Gaussian differentiates as
-//   d/dA_x phi_a = 2 alpha phi_{a+1x} - a_x phi_{a-1x}
-// (Obara-Saika 1986, Eq. 5; eri.py:85-175 of the reference generator), so the
-// bra Hermite range grows by one level (R up to L + 1, X_e up to LA + LB + 1)
-// and the epilogue sums E^{a+-1,b} and E^{a,b+-1} against X:
-//   dJ_ab/dA_x = S_ab sum_e (2 alpha E^{a+1x,b}_e - a_x E^{a-1x,b}_e) X_e,
-// the same with beta = p - alpha on B.  Output: mat_J[k * gstride + o],
-// k = 0..2 the A components, 3..5 the B components, accumulated with +=.
-// The library's gradient entry points use coulomb_grad_kernel
-// (jgrad_kernels.cuh), the same mathematics with several quartets per warp;
-// this one-quartet-per-warp form is not dispatched.
+// The nuclear-gradient form of the same mathematics (bra Hermite range one
+// level higher, derivative epilogue) is coulomb_grad_kernel in
+// jgrad_kernels.cuh.
 #pragma once
 #include <type_traits>
 
@@ -35,19 +25,19 @@ namespace vlxb {
 
 constexpr int MD_THREADS = 128;
 
-template <int LA, int LB, int LC, int LD, int PM, int G = 0>
+template <int LA, int LB, int LC, int LD, int PM>
 __global__ void __launch_bounds__(MD_THREADS)
 coulomb_md_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, double thr, BoysTabs tabs,
-                  unsigned long long* __restrict__ qcount, double fp32_cut, int64_t gstride)
+                  unsigned long long* __restrict__ qcount, double fp32_cut, double fp32_budget)
 {
     using T = typename std::conditional<PM == 0, double, float>::type;
-    constexpr int L = LA + LB + LC + LD + G;
-    constexpr int NHB = nherm(LA + LB + G), NHK = nherm(LC + LD), NHL = nherm(L);
+    constexpr int L = LA + LB + LC + LD;
+    constexpr int NHB = nherm(LA + LB), NHK = nherm(LC + LD), NHL = nherm(L);
     constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     constexpr int NAB = NA * NB, NCD = NC * ND;
     constexpr int NW = MD_THREADS / 32;
     constexpr int NEP = (NHB + 31) / 32;  // bra Hermite indices per lane
-    constexpr int NEK = (LC + 1) * (LD + 1) * (LC + LD + 1), NEB = (LA + 1 + G) * (LB + 1 + G) * (LA + LB + 1 + 2 * G);
+    constexpr int NEK = (LC + 1) * (LD + 1) * (LC + LD + 1), NEB = (LA + 1) * (LB + 1) * (LA + LB + 1);
     __shared__ T sR[NW][2][NHL];
     __shared__ T sDh[NW][NHK];
     __shared__ int16_t sIdx[NHK][NHB];  // index of R_{e+f}
@@ -106,7 +96,7 @@ coulomb_md_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, doubl
         }
         if (threadIdx.x == 0) {
             int ncut, nexact, n64;
-            ket_prefixes(ket, k0, k1, qb, thr, fp32_cut, ncut, nexact, n64);
+            ket_prefixes(ket, k0, k1, qb, thr, fp32_cut, fabs(qb) * pair_amp(b, LB), fp32_budget, ncut, nexact, n64);
             s_ncut = ncut;
             s_n64 = n64;
             if (qcount && PM == 0) atomicAdd(qcount, (unsigned long long)(nexact - k0));
@@ -175,7 +165,7 @@ coulomb_md_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, doubl
                 }
             } else {
                 float F[L + 1];
-                boys_f32<L>(T2, tabs.f32, F);
+                boys_f32<L>(T2, tabs.f64, F);
                 float s = (float)(2.0 * sqrt(rho * INV_PI_D));
                 const float m2r = (float)(-2.0 * rho);
 #pragma unroll
@@ -237,7 +227,7 @@ coulomb_md_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, doubl
         if (threadIdx.x < 3) {
             const double pa = threadIdx.x == 0 ? b.Ax : (threadIdx.x == 1 ? b.Ay : b.Az);
             const double ab = threadIdx.x == 0 ? b.Rx : (threadIdx.x == 1 ? b.Ry : b.Rz);
-            herm_e1_flat<LA + G, LB + G>(pa, pa + ab, b.i2z, sEb[threadIdx.x]);
+            herm_e1_flat<LA, LB>(pa, pa + ab, b.i2z, sEb[threadIdx.x]);
         }
         __syncthreads();
         const uint64_t mask = __ldg(bra.rec_mask + r);
@@ -246,7 +236,7 @@ coulomb_md_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, doubl
             const int ai = c / NB, bi = c % NB;
             const int ax = cart_x(LA, ai), ay = cart_y(LA, ai), az = cart_z(LA, ai);
             const int bx = cart_x(LB, bi), by = cart_y(LB, bi), bz = cart_z(LB, bi);
-            constexpr int LS = LA + LB + 1 + 2 * G, NJ = LB + 1 + G;
+            constexpr int LS = LA + LB + 1, NJ = LB + 1;
             // sum_e E^{(ix,iy,iz),(jx,jy,jz)}_e X_e over the product's Hermite box
             auto hsum = [&](int ix, int iy, int iz, int jx, int jy, int jz) {
                 double acc = 0.0;
@@ -260,23 +250,7 @@ coulomb_md_kernel(JBraRecs bra, JKetPairs ket, double* __restrict__ mat_J, doubl
             };
             const int32_t o = __ldg(bra.entry + c * bra.sp_stride + sp);
             const double S = __ldg(bra.pdata + o);
-            if constexpr (G == 0) {
-                mat_J[o] += S * hsum(ax, ay, az, bx, by, bz);
-            } else {
-                const double al2 = 2.0 * __ldg(bra.geo + G_ALPHA * bra.sp_stride + sp);
-                const double be2 = 2.0 * b.z - al2;
-                const int av[3] = {ax, ay, az}, bv[3] = {bx, by, bz};
-#pragma unroll
-                for (int d = 0; d < 3; d++) {
-                    const int ex = d == 0, ey = d == 1, ez = d == 2;
-                    double gA = al2 * hsum(ax + ex, ay + ey, az + ez, bx, by, bz);
-                    if (av[d] > 0) gA -= av[d] * hsum(ax - ex, ay - ey, az - ez, bx, by, bz);
-                    double gB = be2 * hsum(ax, ay, az, bx + ex, by + ey, bz + ez);
-                    if (bv[d] > 0) gB -= bv[d] * hsum(ax, ay, az, bx - ex, by - ey, bz - ez);
-                    mat_J[d * gstride + o] += S * gA;
-                    mat_J[(3 + d) * gstride + o] += S * gB;
-                }
-            }
+            mat_J[o] += S * hsum(ax, ay, az, bx, by, bz);
         }
         __syncthreads();
     }

@@ -17,6 +17,9 @@
 //    buffer that must start at zero is cleared by the call itself.  Calls that
 //    overlap on the GPU (different streams, or different host threads) race on
 //    the array: serialise them.
+//  * The per-device quartet counters of the other entry points are allocated
+//    on first use, so this path never touches them: its quartets are not
+//    counted (the kernels get a null counter pointer).
 #include <mutex>
 #include <vector>
 

@@ -43,6 +43,7 @@ static std::mutex g_mu;
 static const double* g_boys_dev[64] = {nullptr};
 static const float* g_boys32_dev[64] = {nullptr};
 static std::atomic<double> g_fp32_cut{0.0};
+static std::atomic<double> g_fp32_budget{1e-3};  // recommended: see fp32_budget_get
 
 double fp32_cut_get() { return g_fp32_cut.load(std::memory_order_relaxed); }
 
@@ -50,6 +51,15 @@ int fp32_cut_set(double cut)
 {
     if (!(cut >= 0.0)) return VLXB_EINVAL;
     g_fp32_cut.store(cut);
+    return VLXB_OK;
+}
+
+double fp32_budget_get() { return g_fp32_budget.load(std::memory_order_relaxed); }
+
+int fp32_budget_set(double budget)
+{
+    if (!(budget >= 0.0)) return VLXB_EINVAL;
+    g_fp32_budget.store(budget);
     return VLXB_OK;
 }
 
@@ -182,6 +192,18 @@ static int scan_int(Arena& ar, const int* in, int* out, int64_t n)
     if (!tmp) return VLXB_ENOMEM;
     if (!ar.measuring()) {
         VLXB_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, (int)n, ar.stream()));
+    }
+    return VLXB_OK;
+}
+
+static int inclusive_sum_f64(Arena& ar, const double* in, double* out, int64_t n)
+{
+    size_t bytes = 0;
+    VLXB_CHECK_CUDA(cub::DeviceScan::InclusiveSum(nullptr, bytes, in, out, (int)n, ar.stream()));
+    void* tmp = ar.alloc<char>((int64_t)bytes);
+    if (!tmp) return VLXB_ENOMEM;
+    if (!ar.measuring()) {
+        VLXB_CHECK_CUDA(cub::DeviceScan::InclusiveSum(tmp, bytes, in, out, (int)n, ar.stream()));
     }
     return VLXB_OK;
 }
@@ -676,6 +698,55 @@ int kout_prepare(Arena& ar, int na, int nc, int npa, int npc, const uint32_t* pi
     }
     VLXB_CHECK_CUDA(cudaGetLastError());
     return VLXB_OK;
+}
+
+}  // namespace vlxb
+
+namespace vlxb {
+
+int budget_prefix_records(Arena& ar, PairGroups& g, int npa, int lh)
+{
+    cudaStream_t st = ar.stream();
+    g.rec_qa = ar.alloc<double>(g.rec_stride);
+    g.rec_qpre = ar.alloc<double>(g.rec_stride);
+    if (ar.failed()) return VLXB_ENOMEM;
+    if (!ar.measuring()) {
+        k_rec_amp<<<prep_blocks(g.rec_stride), PREP_THREADS, 0, st>>>(g.n_rec, g.rec_stride, g.rec_sp, g.rec_q,
+                                                                       g.geo, g.sp_stride, lh, g.rec_qa);
+        note_launches();
+    }
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    int rc = inclusive_sum_f64(ar, g.rec_qa, g.rec_qpre, g.rec_stride);
+    if (rc) return rc;
+    if (g.gq) {
+        g.gqa = ar.alloc<double>(g.rec_stride);
+        g.gqpre = ar.alloc<double>(g.rec_stride);
+        if (ar.failed()) return VLXB_ENOMEM;
+        if (!ar.measuring()) {
+            k_grp_amp<<<prep_blocks(g.rec_stride), PREP_THREADS, 0, st>>>(g.gseg + npa, g.rec_stride, g.gbeg, g.gcnt,
+                                                                           g.msp, g.mq, g.geo, g.sp_stride, lh,
+                                                                           g.gqa);
+            note_launches();
+        }
+        VLXB_CHECK_CUDA(cudaGetLastError());
+        rc = inclusive_sum_f64(ar, g.gqa, g.gqpre, g.rec_stride);
+        if (rc) return rc;
+    }
+    return VLXB_OK;
+}
+
+int budget_prefix_kets(Arena& ar, JKetData& kd, int lh)
+{
+    cudaStream_t st = ar.stream();
+    double* amp = ar.alloc<double>(kd.stride);
+    kd.tpre = ar.alloc<double>(kd.stride);
+    if (ar.failed()) return VLXB_ENOMEM;
+    if (!ar.measuring()) {
+        k_jket_amp<<<prep_blocks(kd.stride), PREP_THREADS, 0, st>>>(kd.n, kd.stride, kd.tmax, kd.geo, lh, amp);
+        note_launches();
+    }
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    return inclusive_sum_f64(ar, amp, kd.tpre, kd.stride);
 }
 
 }  // namespace vlxb

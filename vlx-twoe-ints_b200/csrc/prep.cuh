@@ -424,6 +424,60 @@ __global__ void k_kout_maxd(const int* __restrict__ n_blk, const int32_t* __rest
         out[o] = maxD_mol[prim_mol[ish[o]]];
 }
 
+// ------------------------------------------------------------ FP32 error budget
+// FP32 error proxy of a primitive shell pair: its bound times the growth the
+// horizontal recurrence can put on FP32 rounding errors when it moves lh
+// units of angular momentum across the pair, (1 + sqrt(2 zeta) |R|)^lh with
+// R = AB (bra) or CD (ket).  Intermediates of the recurrence scale like
+// |R|^k against the final integral's sqrt(1 / 2 zeta)^k, so rounding errors
+// of the intermediates reach the result multiplied by this factor.
+__device__ __forceinline__ double hrr_amp(const double* __restrict__ geo, int64_t stride, int64_t sp, int lh)
+{
+    if (lh == 0) return 1.0;
+    const double z = geo[G_Z * stride + sp];
+    const double rx = geo[G_RX * stride + sp], ry = geo[G_RY * stride + sp], rz = geo[G_RZ * stride + sp];
+    const double f = 1.0 + sqrt(2.0 * z * (rx * rx + ry * ry + rz * rz));
+    double a = f;
+    for (int k = 1; k < lh; k++) a *= f;
+    return a;
+}
+
+// rec_qa[r] = rec_q[r] * hrr_amp(record r); zero past the live records.
+__global__ void k_rec_amp(const int* __restrict__ n_rec, int64_t stride, const int32_t* __restrict__ rec_sp,
+                          const double* __restrict__ rec_q, const double* __restrict__ geo, int64_t geo_stride,
+                          int lh, double* __restrict__ out)
+{
+    const int n = *n_rec;
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < stride; r += (int64_t)gridDim.x * blockDim.x)
+        out[r] = r < n ? fabs(rec_q[r]) * hrr_amp(geo, geo_stride, rec_sp[r], lh) : 0.0;
+}
+
+// gqa[g] = sum over the group's members of |q| * hrr_amp; zero past the live groups.
+__global__ void k_grp_amp(const int* __restrict__ n_grp, int64_t stride, const int32_t* __restrict__ gbeg,
+                          const int32_t* __restrict__ gcnt, const int32_t* __restrict__ msp,
+                          const double* __restrict__ mq, const double* __restrict__ geo, int64_t geo_stride, int lh,
+                          double* __restrict__ out)
+{
+    const int n = *n_grp;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < stride; t += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        if (t < n) {
+            const int b = gbeg[t], c = gcnt[t];
+            for (int m = b; m < b + c; m++) s += fabs(mq[m]) * hrr_amp(geo, geo_stride, msp[m], lh);
+        }
+        out[t] = s;
+    }
+}
+
+// kamp[t] = tmax[t] * hrr_amp(ket t) over the sorted kets; zero past them.
+__global__ void k_jket_amp(const int* __restrict__ n_sp, int64_t stride, const double* __restrict__ tmax,
+                           const double* __restrict__ geo, int lh, double* __restrict__ out)
+{
+    const int n = *n_sp;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < stride; t += (int64_t)gridDim.x * blockDim.x)
+        out[t] = t < n ? tmax[t] * hrr_amp(geo, stride, t, lh) : 0.0;
+}
+
 // ------------------------------------------------------------ batched Coulomb calls
 // Molecule key of every key-sorted ket (n_mol past the live kets, so they
 // stay last in the stable molecule sort).

@@ -93,6 +93,8 @@ class Lib:
         c.vlxb_fp64Probe.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         c.vlxb_setFp32Cutoff.argtypes = [ctypes.c_double]
         c.vlxb_getFp32Cutoff.restype = ctypes.c_double
+        c.vlxb_setFp32Budget.argtypes = [ctypes.c_double]
+        c.vlxb_getFp32Budget.restype = ctypes.c_double
         c.vlxb_pairsToAO.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_int64, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]
         c.vlxb_fockEnergy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
@@ -160,6 +162,13 @@ class Lib:
 
     def get_fp32_cut(self) -> float:
         return float(self.cdll.vlxb_getFp32Cutoff())
+
+    def set_fp32_budget(self, budget: float):
+        """FP32 error budget (0 = none: the cutoff alone decides)."""
+        self.check(self.cdll.vlxb_setFp32Budget(float(budget)), "vlxb_setFp32Budget")
+
+    def get_fp32_budget(self) -> float:
+        return float(self.cdll.vlxb_getFp32Budget())
 
     def launch_count(self, reset: bool = False) -> int:
         out = ctypes.c_ulonglong(0)

@@ -126,23 +126,38 @@ def _overlap_1d(la, lb, PA, PB, p):
 
 
 def overlap_matrix(mol: Molecule) -> np.ndarray:
+    """AO overlap matrix, one vectorised block per pair of shell types (all
+    shell pairs and primitive pairs of the block at once)."""
     n = mol.naos
     S = np.zeros((n, n))
-    for sa in mol.shells:
-        A = mol.coords[sa.atom]
-        for sb in mol.shells:
-            B = mol.coords[sb.atom]
-            ea = sa.exps[:, None]
-            eb = sb.exps[None, :]
-            p = ea + eb
-            P = (ea[..., None] * A + eb[..., None] * B) / p[..., None]
-            K = np.exp(-ea * eb / p * float(np.sum((A - B) ** 2))) * (math.pi / p) ** 1.5
-            cc = sa.coefs[:, None] * sb.coefs[None, :] * K
-            s1 = [_overlap_1d(sa.l, sb.l, P[..., x] - A[x], P[..., x] - B[x], p) for x in range(3)]
-            for ia, (ax, ay, az) in enumerate(CART[sa.l]):
-                for ib, (bx, by, bz) in enumerate(CART[sb.l]):
-                    v = cc * s1[0][ax, bx] * s1[1][ay, by] * s1[2][az, bz]
-                    S[sa.ao0 + ia, sb.ao0 + ib] = v.sum()
+    by_l = {}
+    for sh in mol.shells:
+        by_l.setdefault(sh.l, []).append(sh)
+    for la, sa in by_l.items():
+        ea = np.array([sh.exps for sh in sa])                # (na, ka)
+        ca = np.array([sh.coefs for sh in sa])
+        A = np.array([mol.coords[sh.atom] for sh in sa])     # (na, 3)
+        ao_a = np.array([sh.ao0 for sh in sa])
+        for lb, sb in by_l.items():
+            eb = np.array([sh.exps for sh in sb])
+            cb = np.array([sh.coefs for sh in sb])
+            B = np.array([mol.coords[sh.atom] for sh in sb])
+            ao_b = np.array([sh.ao0 for sh in sb])
+            # axes: shell a, shell b, primitive a, primitive b
+            a_ = ea[:, None, :, None]
+            b_ = eb[None, :, None, :]
+            p = a_ + b_
+            AB2 = np.sum((A[:, None, :] - B[None, :, :]) ** 2, axis=-1)[:, :, None, None]
+            K = np.exp(-a_ * b_ / p * AB2) * (math.pi / p) ** 1.5
+            cc = ca[:, None, :, None] * cb[None, :, None, :] * K
+            s1 = []
+            for x in range(3):
+                Px = (a_ * A[:, None, None, None, x] + b_ * B[None, :, None, None, x]) / p
+                s1.append(_overlap_1d(la, lb, Px - A[:, None, None, None, x], Px - B[None, :, None, None, x], p))
+            for ia, (ax, ay, az) in enumerate(CART[la]):
+                for ib, (bx, by, bz) in enumerate(CART[lb]):
+                    v = (cc * s1[0][ax, bx] * s1[1][ay, by] * s1[2][az, bz]).sum(axis=(2, 3))
+                    S[np.ix_(ao_a + ia, ao_b + ib)] = v
     return S
 
 

@@ -184,3 +184,22 @@ def set_density(dl: DeviceLists, D: torch.Tensor, stream=None):
             for t, k in enumerate(keys):
                 dl.maxD[k] = float(vals[t])
     return dl
+
+
+def to_host(dl: DeviceLists, mol) -> lists.ReferenceLists:
+    """Host (numpy) copy of device-built lists as a `lists.ReferenceLists`
+    (prim tables from `mol`, which the lists were built from): for the AO
+    contraction on the host and for checks against the CPU references."""
+    pd = lists.prim_data(mol)
+    rl = lists.ReferenceLists(pd=pd, naos=dl.naos, D_AO=dl.D_AO.cpu().numpy(), threshold=dl.threshold,
+                              maxD=dict(dl.maxD))
+    u32 = lambda t: t.cpu().numpy().astype(np.uint32)  # noqa: E731
+    for k, v in dl.j.items():
+        rl.jlists[k] = lists.JList(u32(v["first"]), u32(v["second"]), v["pdata"].cpu().numpy(),
+                                   v["Q"].cpu().numpy(), v["D"].cpu().numpy())
+    for k, v in dl.kpart.items():
+        rl.kpartners[k] = lists.KPartners(u32(v["displs"]), u32(v["counts"]), u32(v["Dinds"]),
+                                          v["Q"].cpu().numpy(), v["pdata"].cpu().numpy())
+    for k, v in dl.kpair.items():
+        rl.kpairs[k] = lists.KPairs(u32(v["i"]), u32(v["k"]))
+    return rl
