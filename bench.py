@@ -25,9 +25,11 @@ After the timed steps the same line carries the other legs (all on this GPU):
            matrices) and against oracle/_ref on the parity rows
   small    5 atoms 3s2p (45 AOs): timed in full on the GPU and on the host
            cores (reference expressions), every value checked
-  large    200 atoms at 25 bohr^3 per atom, 4s3p2d (5000 AOs): incremental
-           build on dD of norm 1e-3, density-weighted screening at 1e-11,
-           mixed precision with FP64 accumulation
+  large    the large sparse recipe (25 bohr^3 per atom, 4s3p2d) at 48 atoms
+           (1200 AOs; --large-atoms 200 runs the 5000-AO cluster, whose
+           incremental build is about 6.4e12 quartets): incremental build on
+           dD of norm 1e-3, density-weighted screening at 1e-11, mixed
+           precision with FP64 accumulation
   batched / served   the batching and serving patterns
   cpu_baseline       the reference's emitted expressions with OpenMP on the
            host cores, a bounded sample of the headline build extrapolated
@@ -87,7 +89,9 @@ def parse():
                     help="mixed-precision leg: FP32 error budget (default: the library's recommended value)")
     ap.add_argument("--schedule", default=None, help="kernel schedule JSON (default: vlxb/schedule_b200.json)")
     ap.add_argument("--small-steps", type=int, default=5, help="5-atom leg: timed builds (0 skips the leg)")
-    ap.add_argument("--large-atoms", type=int, default=200, help="large sparse leg: atoms (0 skips the leg)")
+    ap.add_argument("--large-atoms", type=int, default=48,
+                    help="large sparse leg: atoms at 25 bohr^3/atom (0 skips the leg; 200 is the full cluster, "
+                         "about 6.4e12 quartets per incremental build)")
     ap.add_argument("--pattern-fp32-cut", type=float, default=1e-7,
                     help="batched / served legs: FP32 below this bound (errors reported)")
     ap.add_argument("--batch-mols", type=int, default=32, help="batched leg: molecules (0 skips the leg)")
@@ -461,7 +465,8 @@ def run_large(args, L, dev, stream, cut, budget):
     `cut` inside the error budget and FP64 accumulation, and is added to the
     previous J/K.  Reported: its device time, quartets, screened fraction
     against the full-density lists, errors against the FP64 build of the same
-    dD (AO matrices) and against oracle/_ref on seeded rows."""
+    dD (AO matrices) and against oracle/_ref on seeded rows, and the quartet
+    counts of the reference's screening loops for dD and for the full density."""
     import torch
     from vlxb import basis, devlists, fock, lists
 
@@ -516,10 +521,23 @@ def run_large(args, L, dev, stream, cut, budget):
                             "abs_dE_Eh": abs(lists.energy(dD, J32a, K32a) - lists.energy(dD, J64a, K64a))}
     from oracle import ref
 
-    if ref.available() and args.parity_rows > 0:
-        exp, secs = ref_rows(host, max(2, args.parity_rows // 2), seed=11)
-        res["parity_fp64"] = row_errors(exp, J64, K64) | {"oracle_s": secs}
-        res["parity_mixed"] = row_errors(exp, J32, K32)
+    if ref.available():
+        # the reference's own screening loops: the quartet count of the dD
+        # build (must equal the kernels' counters) and of a full-density build
+        # of the same molecule, whose ratio is the screened fraction
+        q_ref = quartets_per_build_ref(host)
+        with torch.cuda.stream(stream):
+            dl0 = devlists.build_device_lists(wl.mol, wl.D, 1e-11, dev)
+            torch.cuda.synchronize()
+        host0 = devlists.to_host(dl0, wl.mol)
+        del dl0
+        q_full = quartets_per_build_ref(host0)
+        res["screening"] = {"quartets_dD_reference_count": q_ref, "counts_equal": q_ref == q,
+                            "quartets_full_density": q_full, "fraction_kept": q / q_full if q_full else None}
+        if args.parity_rows > 0:
+            exp, secs = ref_rows(host, max(2, args.parity_rows // 2), seed=11)
+            res["parity_fp64"] = row_errors(exp, J64, K64) | {"oracle_s": secs}
+            res["parity_mixed"] = row_errors(exp, J32, K32)
     return res
 
 

@@ -223,6 +223,44 @@ def test_edge_cases_empty_and_invalid():
     assert float(out2.abs().max()) == 0.0
 
 
+def test_tma_staged_coulomb_matches_thread_kernel():
+    """J variant 3 (the ket stream staged into shared memory by TMA bulk
+    copies) against variant 0 on ket lists of several tiles, in FP64 and with
+    an FP32 pass (whose ket ranges start at odd positions, so the copies start
+    one ket early): same J to rounding, the same quartet counts, and no
+    bounded wait ran out."""
+    L = lib()
+    L.init(0)
+    wl = basis.config_custom(4, 5.0, {0: 2, 1: 2, 2: 1}, 3, 0.1, 2.5, 4, 1e-12, 37)
+    rl = lists.build_lists(wl.mol, wl.D, wl.threshold, fock.gpu_schwarz_fn())
+    assert max(len(v.first) for v in rl.jlists.values()) > 4 * 128
+    dl = fock.to_device(rl)
+    saved = {c: L.get_schedule("J", c) for c in lists.j_classes()}
+    budget = L.get_fp32_budget()
+    L.kernel_errors(reset=True)
+    try:
+        L.set_fp32_budget(0.0)
+        for cut in (0.0, 1e-6):
+            res = {}
+            for v in (0, 3):
+                for c in lists.j_classes():
+                    L.set_schedule("J", c, v)
+                L.set_fp32_cut(cut)
+                L.reset_counters()
+                mJ, _ = fock.build_jk(dl, do_k=False)
+                torch.cuda.synchronize()
+                res[v] = ({k: t.cpu().numpy() for k, t in mJ.items()}, L.quartet_counters(reset=True)[0])
+            for k in res[0][0]:
+                assert close(res[3][0][k], res[0][0][k]), (cut, k)
+            assert res[3][1] == res[0][1]
+    finally:
+        L.set_fp32_cut(0.0)
+        L.set_fp32_budget(budget)
+        for c, v in saved.items():
+            L.set_schedule("J", c, v)
+    assert L.kernel_errors() == 0
+
+
 def _k_variants(cls):
     """Exchange variants compiled for a class (column ones only when their
     shared memory fits; the library falls back to the thread kernel)."""
@@ -240,10 +278,10 @@ def _k_variants(cls):
     return out
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
 def test_golden_every_coulomb_variant(golden, variant):
-    """Every Coulomb kernel (thread per quartet, warp column, McMurchie-Davidson)
-    on every class."""
+    """Every Coulomb kernel (thread per quartet, warp column, McMurchie-Davidson,
+    thread per quartet with TMA-staged kets) on every class."""
     z = golden
     L = lib()
     saved = {c: L.get_schedule("J", c) for c in tf.j_classes()}

@@ -1,9 +1,12 @@
 // Per-class host drivers: regroup the caller's lists on the device, then
 // launch the class's integral kernel, all on the caller's stream.
 #pragma once
+#include <atomic>
+
 #include "col_kernels.cuh"
 #include "engine.cuh"
 #include "jk_kernels.cuh"
+#include "jtma_kernels.cuh"
 #include "md_kernels.cuh"
 #include "jgrad_kernels.cuh"
 #include "kgrad_kernels.cuh"
@@ -60,6 +63,26 @@ struct ExchangeArgs {
     const double* maxD_mol;         // [molecules] max |D| bound of each molecule
 };
 
+// The staged Coulomb kernel's shared memory exceeds the 48 KB default for
+// kets with d functions: raise the limit once per device for each of its
+// two instantiations.
+template <int LA, int LB, int LC, int LD>
+int jtma_prepare_launch()
+{
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    VLXB_CHECK_CUDA(cudaGetDevice(&dev));
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return VLXB_OK;
+    const int smem = (int)JTmaShape<LC, LD>::SMEM;
+    VLXB_CHECK_CUDA(cudaFuncSetAttribute(coulomb_tma_kernel<LA, LB, LC, LD, 0>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    VLXB_CHECK_CUDA(cudaFuncSetAttribute(coulomb_tma_kernel<LA, LB, LC, LD, 1>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    done.fetch_or(bit, std::memory_order_acq_rel);
+    return VLXB_OK;
+}
+
 // Coulomb class call on a given arena (pool, static or measuring) with given
 // Boys tables and quartet counter (may be null).  G = 1: the bra-centre
 // derivatives of J instead (coulomb_grad_kernel), written to
@@ -111,6 +134,8 @@ int run_coulomb_impl(const CoulombArgs& a, cudaStream_t st, Arena& ar, const Boy
                   kd.Dh, kd.tpre};
     int grid = launch_grid_limit();
     if ((int64_t)grid > (int64_t)a.n_ab) grid = (int)a.n_ab;
+    unsigned long long* kerr = kernel_errors_device();
+    if (jvar == 3 && !kerr) return VLXB_ECUDA;
     for (int pm = 0; pm < (cut > 0.0 ? 2 : 1); pm++) {
         if constexpr (G == 1) {
             constexpr int GT = JGradShape<LA, LB, LC, LD>::THREADS;
@@ -127,6 +152,16 @@ int run_coulomb_impl(const CoulombArgs& a, cudaStream_t st, Arena& ar, const Boy
             else
                 coulomb_md_kernel<LA, LB, LC, LD, 1><<<grid, MD_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc,
                                                                                   cut, budget);
+        } else if (jvar == 3) {
+            using JS = JTmaShape<LC, LD>;
+            int rc2 = jtma_prepare_launch<LA, LB, LC, LD>();
+            if (rc2) return rc2;
+            if (pm == 0)
+                coulomb_tma_kernel<LA, LB, LC, LD, 0><<<grid, JT_TILE, JS::SMEM, st>>>(bra, ket, a.mat_J, a.thr, tab,
+                                                                                      qc, cut, budget, kerr);
+            else
+                coulomb_tma_kernel<LA, LB, LC, LD, 1><<<grid, JT_TILE, JS::SMEM, st>>>(bra, ket, a.mat_J, a.thr, tab,
+                                                                                      qc, cut, budget, kerr);
         } else if (jvar == 1) {
             if (pm == 0)
                 coulomb_col_kernel<LA, LB, LC, LD, 0><<<grid, J_THREADS, 0, st>>>(bra, ket, a.mat_J, a.thr, tab, qc,

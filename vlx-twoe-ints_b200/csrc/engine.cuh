@@ -116,6 +116,9 @@ int fp32_budget_set(double budget);
 // Per-device counters of screened-in primitive shell quartets processed by
 // the J ([0]) and K ([1]) kernels (device memory, allocated with the table).
 unsigned long long* quartet_counters_device();
+// Per-device kernel error word (flags VLXB_KERR_*, OR-ed in by kernels whose
+// bounded waits ran out); the word after the two counters.
+unsigned long long* kernel_errors_device();
 
 // Make the device's default memory pool keep freed scratch (release
 // threshold = max) so per-call scratch costs no new cudaMalloc after warm-up.

@@ -147,6 +147,12 @@ def header():
          "   (2 values; synchronises `stream`) when host_out is not NULL, then zeroes",
          "   the counters when reset != 0.  No reference counterpart. */",
          "int vlxb_quartetCounters(unsigned long long* host_out, int reset, void* stream);", "",
+         "/* Device error word of the kernels (flags OR-ed in on the device): bit 0 =",
+         "   a bulk copy into shared memory (J schedule variant 3) did not land within",
+         "   its bounded wait; the kernel then stopped without finishing its work.",
+         "   Reads it into *host_out (if non-NULL, synchronising `stream`) and zeroes it",
+         "   if `reset`.  No reference counterpart. */",
+         "int vlxb_kernelErrors(unsigned long long* host_out, int reset, void* stream);", "",
          "/* Number of this library's own kernel launches since the last reset",
          "   (host-side count; reset != 0 zeroes it after reading).  No reference",
          "   counterpart. */",
@@ -158,7 +164,9 @@ def header():
          "int vlxb_fp64Probe(double* out, int iters, int blocks, void* stream);", "",
          "/* Kernel variant used for one class (kind 0 = Coulomb: 0 one thread per",
          "   shell quartet, 1 warp-cooperative column kernel, 2 McMurchie-Davidson",
-         "   kernel (Hermite ket densities, one quartet per warp); kind 1 = exchange: 0",
+         "   kernel (Hermite ket densities, one quartet per warp), 3 one thread per",
+         "   quartet with the sorted ket stream staged into shared memory by TMA bulk",
+         "   copies, double-buffered; kind 1 = exchange: 0",
          "   one thread per quartet, 1 column kernel with bra lanes, 2 column kernel",
          "   with ket lanes, 3 / 4 the column kernels with bra / ket lanes that sum",
          "   the primitive partners of one contracted shell before the HRR).  A",
@@ -175,7 +183,7 @@ def header():
          "   behaviour.  Process-wide.  No reference counterpart. */",
          "int vlxb_setFp32Cutoff(double cutoff);",
          "double vlxb_getFp32Cutoff(void);", "",
-         "/* FP32 error budget (with a cutoff > 0; default 1e-3; 0 = no budget, the",
+         "/* FP32 error budget (with a cutoff > 0; default 2; 0 = no budget, the",
          "   cutoff alone decides).  A quartet below the cutoff runs in FP32 only inside the tail",
          "   of its list whose summed error proxy stays within `budget`: per J bra",
          "   record, |Q_ij| A_ij * sum over the FP32 kets of max|Q_kl D_kl| A_kl; per",

@@ -43,7 +43,7 @@ static std::mutex g_mu;
 static const double* g_boys_dev[64] = {nullptr};
 static const float* g_boys32_dev[64] = {nullptr};
 static std::atomic<double> g_fp32_cut{0.0};
-static std::atomic<double> g_fp32_budget{1e-3};  // recommended: see fp32_budget_get
+static std::atomic<double> g_fp32_budget{2.0};
 
 double fp32_cut_get() { return g_fp32_cut.load(std::memory_order_relaxed); }
 
@@ -98,11 +98,17 @@ unsigned long long* quartet_counters_device()
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_counters[dev]) {
         unsigned long long* p = nullptr;
-        if (cudaMalloc(&p, 2 * sizeof(unsigned long long)) != cudaSuccess) return nullptr;
-        if (cudaMemset(p, 0, 2 * sizeof(unsigned long long)) != cudaSuccess) return nullptr;
+        if (cudaMalloc(&p, 4 * sizeof(unsigned long long)) != cudaSuccess) return nullptr;
+        if (cudaMemset(p, 0, 4 * sizeof(unsigned long long)) != cudaSuccess) return nullptr;
         g_counters[dev] = p;
     }
     return g_counters[dev];
+}
+
+unsigned long long* kernel_errors_device()
+{
+    unsigned long long* p = quartet_counters_device();
+    return p ? p + 2 : nullptr;
 }
 
 const double* boys_table_device()
@@ -161,7 +167,7 @@ int schedule_set(int kind, int la, int lb, int lc, int ld, int variant)
 {
     if (kind < 0 || kind > 1 || la < 0 || la > 2 || lb < 0 || lb > 2 || lc < 0 || lc > 2 || ld < 0 || ld > 2)
         return VLXB_EINVAL;
-    if (variant < 0 || variant > (kind == 0 ? 2 : 4)) return VLXB_EINVAL;
+    if (variant < 0 || variant > (kind == 0 ? 3 : 4)) return VLXB_EINVAL;
     std::call_once(g_sched_once, sched_init);
     g_sched[kind][la * 27 + lb * 9 + lc * 3 + ld].store(variant);
     return VLXB_OK;
@@ -539,15 +545,18 @@ int jket_prepare(Arena& ar, const PairGroups& g, const uint32_t* first, const ui
     double* Dm_u = ar.alloc<double>(S * NCD);
     double* Qc_u = ar.alloc<double>(S * NCD);
     double* Dc_u = ar.alloc<double>(S * NCD);
-    out.geo = ar.alloc<double>(S * GEO_N);
-    out.tmin = ar.alloc<double>(S);
-    out.tmax = ar.alloc<double>(S);
-    out.Dpp = ar.alloc<double>(S * NF);
-    out.Dm = ar.alloc<double>(S * NCD);
-    out.Qc = ar.alloc<double>(S * NCD);
-    out.Dc = ar.alloc<double>(S * NCD);
+    // the sorted ket arrays get an even row stride, so that every row of
+    // them starts on a 16-byte boundary (bulk copies into shared memory)
+    const int64_t SA = (S + 1) & ~(int64_t)1;
+    out.geo = ar.alloc<double>(SA * GEO_N);
+    out.tmin = ar.alloc<double>(SA);
+    out.tmax = ar.alloc<double>(SA);
+    out.Dpp = ar.alloc<double>(SA * NF);
+    out.Dm = ar.alloc<double>(SA * NCD);
+    out.Qc = ar.alloc<double>(SA * NCD);
+    out.Dc = ar.alloc<double>(SA * NCD);
     if (ar.failed()) return VLXB_ENOMEM;
-    out.stride = S;
+    out.stride = SA;
     out.n = g.n_sp;
     if (!ar.measuring()) {
         k_jket_fill<LC, LD><<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, g.entry, S, first, second, D, Q, pdata,
@@ -597,17 +606,17 @@ int jket_prepare(Arena& ar, const PairGroups& g, const uint32_t* first, const ui
         keys_sorted = keys_c;
     }
     if (!ar.measuring()) {
-        k_jket_gather<LC, LD><<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, perm, S, g.geo, keys_sorted, tmin_u,
+        k_jket_gather<LC, LD><<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, perm, S, SA, g.geo, keys_sorted, tmin_u,
                                                                        Dpp_u, Dm_u, Qc_u, Dc_u, out.geo, out.tmax,
                                                                        out.tmin, out.Dpp, out.Dm, out.Qc, out.Dc);
     }
     if (!ar.measuring()) note_launches();
     VLXB_CHECK_CUDA(cudaGetLastError());
     if (hermite) {
-        out.Dh = ar.alloc<double>(S * nherm(LC + LD));
+        out.Dh = ar.alloc<double>(SA * nherm(LC + LD));
         if (!out.Dh) return VLXB_ENOMEM;
         if (!ar.measuring()) {
-            k_jket_hermite<LC, LD><<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, S, out.geo, out.Dm, out.Dh);
+            k_jket_hermite<LC, LD><<<prep_blocks(S), PREP_THREADS, 0, st>>>(g.n_sp, SA, out.geo, out.Dm, out.Dh);
             note_launches();
         }
         VLXB_CHECK_CUDA(cudaGetLastError());

@@ -286,7 +286,7 @@ __global__ void k_jket_fill(const int* __restrict__ n_sp, const int32_t* __restr
 // Gather ket arrays into the sorted order given by perm.
 template <int LC, int LD>
 __global__ void k_jket_gather(const int* __restrict__ n_sp, const int* __restrict__ perm, int64_t stride,
-                              const double* __restrict__ geo_in, const double* __restrict__ tmax_in,
+                              int64_t ostride, const double* __restrict__ geo_in, const double* __restrict__ tmax_in,
                               const double* __restrict__ tmin_in, const double* __restrict__ Dpp_in,
                               const double* __restrict__ Dm_in, const double* __restrict__ Qc_in,
                               const double* __restrict__ Dc_in, double* __restrict__ geo, double* __restrict__ tmax,
@@ -297,14 +297,14 @@ __global__ void k_jket_gather(const int* __restrict__ n_sp, const int* __restric
     const int n = *n_sp;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
         const int p = perm[r];
-        for (int g = 0; g < GEO_N; g++) geo[g * stride + r] = geo_in[g * stride + p];
+        for (int g = 0; g < GEO_N; g++) geo[g * ostride + r] = geo_in[g * stride + p];
         tmax[r] = tmax_in[r];  // keys are already sorted
         tmin[r] = tmin_in[p];
-        for (int f = 0; f < NF; f++) Dpp[f * stride + r] = Dpp_in[f * stride + p];
+        for (int f = 0; f < NF; f++) Dpp[f * ostride + r] = Dpp_in[f * stride + p];
         for (int c = 0; c < NCD; c++) {
-            Dm[c * stride + r] = Dm_in[c * stride + p];
-            Qc[c * stride + r] = Qc_in[c * stride + p];
-            Dc[c * stride + r] = Dc_in[c * stride + p];
+            Dm[c * ostride + r] = Dm_in[c * stride + p];
+            Qc[c * ostride + r] = Qc_in[c * stride + p];
+            Dc[c * ostride + r] = Dc_in[c * stride + p];
         }
     }
 }

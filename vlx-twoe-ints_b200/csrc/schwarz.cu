@@ -81,3 +81,17 @@ extern "C" int vlxb_quartetCounters(unsigned long long* host_out, int reset, voi
     if (reset) VLXB_CHECK_CUDA(cudaMemsetAsync(qc, 0, 2 * sizeof(unsigned long long), st));
     return VLXB_OK;
 }
+
+extern "C" int vlxb_kernelErrors(unsigned long long* host_out, int reset, void* stream)
+{
+    using namespace vlxb;
+    unsigned long long* e = kernel_errors_device();
+    if (!e) return VLXB_ECUDA;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (host_out) {
+        VLXB_CHECK_CUDA(cudaMemcpyAsync(host_out, e, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        VLXB_CHECK_CUDA(cudaStreamSynchronize(st));
+    }
+    if (reset) VLXB_CHECK_CUDA(cudaMemsetAsync(e, 0, sizeof(unsigned long long), st));
+    return VLXB_OK;
+}

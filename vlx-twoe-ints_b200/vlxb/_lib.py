@@ -87,6 +87,7 @@ class Lib:
                                           ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                           ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
         c.vlxb_quartetCounters.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        c.vlxb_kernelErrors.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         c.vlxb_setSchedule.argtypes = [ctypes.c_int] * 6
         c.vlxb_getSchedule.argtypes = [ctypes.c_int] * 5
         c.vlxb_launchCount.argtypes = [ctypes.c_void_p, ctypes.c_int]
@@ -198,6 +199,12 @@ class Lib:
     def block_max_abs(self, D, naos, rows, nrows, cols, ncols, out, stream: int = 0):
         self.check(self.cdll.vlxb_blockMaxAbs(D, int(naos), rows, int(nrows), cols, int(ncols), out, stream),
                    "vlxb_blockMaxAbs")
+
+    def kernel_errors(self, reset: bool = False, stream: int = 0) -> int:
+        """Device error word of the kernels (0 = no bounded wait ran out)."""
+        out = ctypes.c_ulonglong(0)
+        self.check(self.cdll.vlxb_kernelErrors(ctypes.byref(out), int(reset), stream), "vlxb_kernelErrors")
+        return int(out.value)
 
     def reset_counters(self, stream: int = 0):
         self.check(self.cdll.vlxb_quartetCounters(None, 1, stream), "vlxb_quartetCounters")

@@ -29,7 +29,7 @@ ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v", "-I", CSRC] + ARCH_FLAGS
 
 COMMON_HEADERS = ["common.cuh", "engine.cuh", "jk_kernels.cuh", "prep.cuh", "classes.cuh", "col_kernels.cuh",
-                  "md.cuh", "md_kernels.cuh", "jgrad_kernels.cuh", "kgrad_kernels.cuh"]
+                  "md.cuh", "md_kernels.cuh", "jgrad_kernels.cuh", "kgrad_kernels.cuh", "tma.cuh", "jtma_kernels.cuh"]
 
 
 def _run_generators():

@@ -1,6 +1,7 @@
 """Autotuner: pick the kernel variant of every J and K class by timing.
 
-For each class and each compiled variant (J: thread-per-quartet, column;
+For each class and each compiled variant (J: thread-per-quartet, column,
+McMurchie-Davidson, thread-per-quartet with TMA-staged kets;
 K: thread-per-quartet, column with bra lanes, column with ket lanes) the class
 entry point is timed with CUDA events on a given system's lists (best of
 `reps`), and the fastest variant is kept.  The result is a JSON schedule
@@ -37,7 +38,7 @@ def compiled_variants(kind: str, cls: str):
     from gen_column import ColumnPlan, k_smem_bytes
 
     if kind == "J":
-        return [1, 2] if cls in SPILLING_THREAD_KERNELS["J"] else [0, 1, 2]
+        return [1, 2] if cls in SPILLING_THREAD_KERNELS["J"] else [0, 1, 2, 3]
     l = [{"s": 0, "p": 1, "d": 2}[x] for x in cls]
     out = [] if cls in SPILLING_THREAD_KERNELS["K"] else [0]
     for ori in (0, 1):
