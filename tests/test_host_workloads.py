@@ -31,7 +31,7 @@ def test_batch_and_serve_workloads():
 
 
 def test_compiled_variants():
-    assert compiled_variants("J", "ssss") == [0, 1, 2]
+    assert compiled_variants("J", "ssss") == [0, 1, 2, 3]
     assert 0 not in compiled_variants("J", "dddd")  # its thread kernel spills and is never timed
     kv = compiled_variants("K", "pddd")
     assert set(kv) <= {0, 1, 2, 3, 4} and {1, 3} <= set(kv)
