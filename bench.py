@@ -30,7 +30,8 @@ After the timed steps the same line carries the other legs (all on this GPU):
            incremental build is about 6.4e12 quartets): incremental build on
            dD of norm 1e-3, density-weighted screening at 1e-11, mixed
            precision with FP64 accumulation
-  batched / served   the batching and serving patterns
+  batched / served   the batching and serving patterns (served: one rate
+           below the plain server's capacity and one far above it)
   cpu_baseline       the reference's emitted expressions with OpenMP on the
            host cores, a bounded sample of the headline build extrapolated
 
@@ -43,6 +44,9 @@ Tool modes (no driver line; used by the profiles under profiles/):
         nuclear-gradient entry points against the J / K builds
     python bench.py --mode gradient-cpu [--atoms 10]
         CPU baseline of the nuclear gradients (oracle port, no GPU)
+    python bench.py --mode large|batched|served [leg options]
+        one leg alone at the sizes given (e.g. --large-atoms 200 --large-no-fp64,
+        --batch-mols 256 --batch-atoms 3 30), one JSON line
 
 Multi-GPU: the path is a single-GPU build; N GPUs run N independent replicas
 (one process per GPU) and value is the aggregate over the replicas.
@@ -72,7 +76,8 @@ L2_BYTES = 126 * 1024 * 1024
 
 def parse():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--mode", choices=["bench", "case", "classes", "gradient", "gradient-cpu"], default="bench")
+    ap.add_argument("--mode", choices=["bench", "case", "classes", "gradient", "gradient-cpu", "large", "batched",
+                                       "served"], default="bench")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
@@ -92,14 +97,17 @@ def parse():
     ap.add_argument("--large-atoms", type=int, default=48,
                     help="large sparse leg: atoms at 25 bohr^3/atom (0 skips the leg; 200 is the full cluster, "
                          "about 6.4e12 quartets per incremental build)")
-    ap.add_argument("--pattern-fp32-cut", type=float, default=1e-7,
-                    help="batched / served legs: FP32 below this bound (errors reported)")
+    ap.add_argument("--pattern-fp32-cut", type=float, default=1e-6,
+                    help="batched / served legs: FP32 below this bound, inside the FP32 error budget")
+    ap.add_argument("--large-no-fp64", action="store_true",
+                    help="large leg: skip the FP64 reference build (errors against oracle/_ref rows only)")
     ap.add_argument("--batch-mols", type=int, default=32, help="batched leg: molecules (0 skips the leg)")
     ap.add_argument("--batch-atoms", type=int, nargs=2, default=(3, 8), help="batched leg: atom count range")
-    ap.add_argument("--serve-reqs", type=int, default=16, help="served leg: requests (0 skips the leg)")
+    ap.add_argument("--serve-reqs", type=int, default=12, help="served leg: requests per rate (0 skips the leg)")
     ap.add_argument("--serve-atoms", type=int, nargs=2, default=(5, 12), help="served leg: atom count range")
     ap.add_argument("--serve-iters", type=int, default=10, help="served leg: densities per request")
-    ap.add_argument("--serve-rate", type=float, default=50.0, help="served leg: Poisson arrival rate (req/s)")
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=(0.25, 50.0),
+                    help="served leg: Poisson arrival rates (req/s), one run of plain and served per rate")
     # tool modes
     ap.add_argument("--kind", choices=["J", "K"], default="K", help="--mode case: entry-point kind")
     ap.add_argument("--cls", default="pddd", help="--mode case: class")
@@ -493,38 +501,42 @@ def run_large(args, L, dev, stream, cut, budget):
                 t.zero_()
             fock.build_jk(dl, stream=stream, matJ=matJ, matK=matK)
 
-        L.set_fp32_cut(0.0)
-        build()
-        torch.cuda.synchronize()
-        L.reset_counters(stream.cuda_stream)
-        t64 = timed_device(build, 1, stream)[0]
-        qj, qk = L.quartet_counters(reset=True, stream=stream.cuda_stream)
-        J64 = {k: v.cpu().numpy() for k, v in matJ.items()}
-        K64 = {k: v.cpu().numpy() for k, v in matK.items()}
+        # the kernels are loaded by the builds before this leg (or by the
+        # first class calls here), so each build is timed once, cold
+        J64 = K64 = None
+        t64 = None
+        if not args.large_no_fp64:
+            L.set_fp32_cut(0.0)
+            t64 = timed_device(build, 1, stream)[0]
+            J64 = {k: v.cpu().numpy() for k, v in matJ.items()}
+            K64 = {k: v.cpu().numpy() for k, v in matK.items()}
         L.set_fp32_cut(cut)
         L.set_fp32_budget(budget)
-        build()
-        torch.cuda.synchronize()
+        L.reset_counters(stream.cuda_stream)
         tmx = timed_device(build, 1, stream)[0]
+        qj, qk = L.quartet_counters(reset=True, stream=stream.cuda_stream)
         L.set_fp32_cut(0.0)
         J32 = {k: v.cpu().numpy() for k, v in matJ.items()}
         K32 = {k: v.cpu().numpy() for k, v in matK.items()}
     q = qj + qk
-    res.update({"fp64_ms": t64 * 1e3, "mixed_ms": tmx * 1e3, "quartets": q, "value": q / tmx, "unit": UNIT,
-                "builds_per_s": 1.0 / tmx, "speedup_mixed_vs_fp64": t64 / tmx, "fp32_below_bound": cut,
-                "fp32_budget": budget})
+    res.update({"fp64_ms": t64 * 1e3 if t64 else None, "mixed_ms": tmx * 1e3, "quartets": q, "value": q / tmx,
+                "unit": UNIT, "builds_per_s": 1.0 / tmx, "speedup_mixed_vs_fp64": t64 / tmx if t64 else None,
+                "fp32_below_bound": cut, "fp32_budget": budget})
     host = devlists.to_host(dl, wl.mol)
-    J64a, K64a = lists.contract_J(host, J64), lists.contract_K(host, K64)
-    J32a, K32a = lists.contract_J(host, J32), lists.contract_K(host, K32)
-    res["mixed_vs_fp64"] = {"max_abs_dJ": float(np.abs(J32a - J64a).max()),
-                            "max_abs_dK": float(np.abs(K32a - K64a).max()),
-                            "abs_dE_Eh": abs(lists.energy(dD, J32a, K32a) - lists.energy(dD, J64a, K64a))}
+    if J64 is not None:
+        J64a, K64a = lists.contract_J(host, J64), lists.contract_K(host, K64)
+        J32a, K32a = lists.contract_J(host, J32), lists.contract_K(host, K32)
+        res["mixed_vs_fp64"] = {"max_abs_dJ": float(np.abs(J32a - J64a).max()),
+                                "max_abs_dK": float(np.abs(K32a - K64a).max()),
+                                "abs_dE_Eh": abs(lists.energy(dD, J32a, K32a) - lists.energy(dD, J64a, K64a))}
     from oracle import ref
 
-    if ref.available():
+    if ref.available() and wl.mol.naos <= 2400:
         # the reference's own screening loops: the quartet count of the dD
         # build (must equal the kernels' counters) and of a full-density build
-        # of the same molecule, whose ratio is the screened fraction
+        # of the same molecule, whose ratio is the screened fraction (host
+        # counting time grows past minutes beyond ~2400 AOs, so larger
+        # clusters skip it)
         q_ref = quartets_per_build_ref(host)
         with torch.cuda.stream(stream):
             dl0 = devlists.build_device_lists(wl.mol, wl.D, 1e-11, dev)
@@ -534,10 +546,11 @@ def run_large(args, L, dev, stream, cut, budget):
         q_full = quartets_per_build_ref(host0)
         res["screening"] = {"quartets_dD_reference_count": q_ref, "counts_equal": q_ref == q,
                             "quartets_full_density": q_full, "fraction_kept": q / q_full if q_full else None}
-        if args.parity_rows > 0:
-            exp, secs = ref_rows(host, max(2, args.parity_rows // 2), seed=11)
+    if ref.available() and args.parity_rows > 0:
+        exp, secs = ref_rows(host, max(2, args.parity_rows // 2), seed=11)
+        if J64 is not None:
             res["parity_fp64"] = row_errors(exp, J64, K64) | {"oracle_s": secs}
-            res["parity_mixed"] = row_errors(exp, J32, K32)
+        res["parity_mixed"] = row_errors(exp, J32, K32) | {"oracle_s": secs}
     return res
 
 
@@ -622,43 +635,79 @@ def run_batched(args, L, dev, cut):
 def run_served(args, L, dev, cut):
     """Served leg: Poisson arrivals, atom counts log-uniform, each request a
     sequence of densities (D0 then D0 + seeded perturbations of norm 1e-2 ..
-    1e-6).  plain = one request at a time, full FP64 builds; served =
-    continuous admission of up to 8 concurrent requests on their own streams,
-    FP32 below `cut`, incremental dD builds.  Wall-clock (host) timing of the
-    whole request stream; p50/p99 = request latency from arrival to result."""
+    1e-6).  Per arrival rate: plain = one request at a time, full FP64
+    builds; served = continuous admission of up to 8 concurrent requests on
+    their own streams, FP32 below `cut` inside the FP32 error budget,
+    incremental dD builds.  Wall-clock (host) timing of the whole request
+    stream; p50/p99 = request latency from arrival to result.  One rate sits
+    below the plain server's capacity (latency = service time) and one far
+    above it (latency dominated by queueing)."""
     from vlxb import basis
     from vlxb.serve import Request, Server, perturbed_densities
 
     counts = basis.serve_atom_counts(args.serve_reqs, args.serve_atoms[0], args.serve_atoms[1], seed=5)
     wls = [basis.molecule_at_density(int(n), 30.0, 1000 + t) for t, n in enumerate(counts)]
-    rng = np.random.default_rng(11)
-    gaps = rng.exponential(1.0 / args.serve_rate, size=len(wls))
-    arr = np.cumsum(gaps) - gaps[0]
 
-    def reqs():
+    def reqs(arr):
         out = []
         for t, w in enumerate(wls):
             Ds = perturbed_densities(w.D, args.serve_iters, np.random.default_rng(200 + t))
             out.append(Request(t, w.mol, Ds, w.threshold, arrival=float(arr[t])))
         return out
 
-    Server(device=dev, max_active=1).run(reqs()[:1])  # warm-up (kernel loading)
-    plain = Server(device=dev, max_active=1).run(reqs())
-    fast_reqs = reqs()
-    fast = Server(device=dev, max_active=8, fp32_cut=cut, incremental=True).run(fast_reqs)
-    ref_reqs = reqs()
-    Server(device=dev, max_active=8).run(ref_reqs)
-    dE = max(abs(a.energies[-1] - b.energies[-1]) for a, b in zip(fast_reqs, ref_reqs))
-    dJ = max(float(np.abs(a.J - b.J).max()) for a, b in zip(fast_reqs, ref_reqs))
-    dK = max(float(np.abs(a.K - b.K).max()) for a, b in zip(fast_reqs, ref_reqs))
-    return {"requests": len(wls), "atoms": [int(counts.min()), int(counts.max())],
-            "densities_per_request": args.serve_iters, "rate_req_per_s": args.serve_rate,
-            "plain_fp64": {k: plain[k] for k in ("builds_per_s", "p50_ms", "p99_ms", "wall_s")},
-            "served_mixed_incremental": {k: fast[k] for k in ("builds_per_s", "p50_ms", "p99_ms", "wall_s")},
-            "speedup_builds_per_s": fast["builds_per_s"] / plain["builds_per_s"], "fp32_below_bound": cut,
-            "max_abs_dJ_last": dJ, "max_abs_dK_last": dK, "abs_dE_last_Eh": dE,
-            "reference": "the same request stream served with full FP64 builds",
+    Server(device=dev, max_active=1).run(reqs(np.zeros(len(wls)))[:1])  # warm-up (kernel loading)
+    keys = ("builds_per_s", "p50_ms", "p99_ms", "wall_s")
+    per_rate = []
+    err = None
+    for rate in args.serve_rates:
+        rng = np.random.default_rng(11)
+        gaps = rng.exponential(1.0 / rate, size=len(wls))
+        arr = np.cumsum(gaps) - gaps[0]
+        plain = Server(device=dev, max_active=1).run(reqs(arr))
+        fast_reqs = reqs(arr)
+        fast = Server(device=dev, max_active=8, fp32_cut=cut, incremental=True).run(fast_reqs)
+        per_rate.append({"rate_req_per_s": rate, "plain_fp64": {k: plain[k] for k in keys},
+                         "served_mixed_incremental": {k: fast[k] for k in keys},
+                         "speedup_builds_per_s": fast["builds_per_s"] / plain["builds_per_s"]})
+        if err is None:
+            ref_reqs = reqs(arr)
+            Server(device=dev, max_active=8).run(ref_reqs)
+            err = {"max_abs_dJ_last": max(float(np.abs(a.J - b.J).max()) for a, b in zip(fast_reqs, ref_reqs)),
+                   "max_abs_dK_last": max(float(np.abs(a.K - b.K).max()) for a, b in zip(fast_reqs, ref_reqs)),
+                   "abs_dE_last_Eh": max(abs(a.energies[-1] - b.energies[-1])
+                                         for a, b in zip(fast_reqs, ref_reqs))}
+    return {"requests_per_rate": len(wls), "atoms": [int(counts.min()), int(counts.max())],
+            "densities_per_request": args.serve_iters, "fp32_below_bound": cut,
+            "fp32_budget": L.get_fp32_budget(), "rates": per_rate, **(err or {}),
+            "reference": "the same request stream served with full FP64 builds (errors: first rate)",
             "timing": "wall clock of the whole request stream (host-side serving loop included)"}
+
+
+def run_leg(args):
+    """One leg alone (--mode large / batched / served) at the sizes given."""
+    import torch
+    from vlxb._lib import lib
+    from vlxb.tune import DEFAULT_SCHEDULE, apply_schedule
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    L = lib()
+    L.init(0)
+    apply_schedule(args.schedule or DEFAULT_SCHEDULE)
+    if args.fp32_budget is not None:
+        L.set_fp32_budget(args.fp32_budget)
+    stream = torch.cuda.Stream(device=dev)
+    t0 = time.perf_counter()
+    if args.mode == "large":
+        res = run_large(args, L, dev, stream, args.fp32_cut, L.get_fp32_budget())
+    elif args.mode == "batched":
+        res = run_batched(args, L, dev, args.pattern_fp32_cut)
+    else:
+        res = run_served(args, L, dev, args.pattern_fp32_cut)
+    res["leg"] = args.mode
+    res["wall_s_total"] = time.perf_counter() - t0
+    print(json.dumps(res))
+    return 0
 
 
 # ----------------------------------------------------------------- our arm
@@ -1132,6 +1181,8 @@ def main():
         return mode_classes(args)
     if args.mode == "gradient":
         return mode_gradient(args)
+    if args.mode in ("large", "batched", "served"):
+        return run_leg(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -211,6 +211,14 @@ static OrCtx* ctx_new_nb(int nb)
 
 static OrCtx* ctx_new(void) { return ctx_new_nb(OR_MAXL + 1); }
 
+/* Context large enough for a class: Cartesian exponents of e = a + b and
+   f = c + d reach la + lb and lc + ld (up to 6 with f shells). */
+static OrCtx* ctx_for(int la, int lb, int lc, int ld)
+{
+    int emax = (la + lb > lc + ld) ? la + lb : lc + ld;
+    return ctx_new_nb(emax + 1 > OR_MAXL + 1 ? emax + 1 : OR_MAXL + 1);
+}
+
 static void ctx_free(OrCtx* c) { free(c->memo); free(c->stamp); free(c); }
 
 /* Cartesian component tables, in the reference's order (gen_coulomb.py:143-148):
@@ -310,7 +318,8 @@ static inline void prim_of(const double* info, uint32_t count, int l, uint32_t i
 }
 
 /* J of one (ab|cd) class in prim-cart pair space (gen_coulomb.py:74-297).
-   prim_info[l] / prim_count[l] for l = 0,1,2 (entries for unused l ignored).
+   prim_info[l] / prim_count[l] for l = 0..3 (s, p, d, f; entries for unused
+   l ignored).
    rows: optional subset of bra indices (NULL = all); results go to mat_J[ij]
    with +=, as the emitted kernel does. */
 void oracle_coulomb_fock(int la, int lb, int lc, int ld, double* mat_J,
@@ -326,7 +335,7 @@ void oracle_coulomb_fock(int la, int lb, int lc, int ld, double* mat_J,
     int L = la + lb + lc + ld;
     #pragma omp parallel
     {
-        OrCtx* c = ctx_new();
+        OrCtx* c = ctx_for(la, lb, lc, ld);
         #pragma omp for schedule(dynamic, 4)
         for (int64_t w = 0; w < (int64_t)nwork; w++) {
             uint32_t ij = rows ? rows[w] : (uint32_t)w;
@@ -439,7 +448,7 @@ void oracle_exchange_fock(int la, int lb, int lc, int ld, double* mat_K,
     int ncb = ncart_of[lb], ncd = ncart_of[ld];
     #pragma omp parallel
     {
-        OrCtx* c = ctx_new();
+        OrCtx* c = ctx_for(la, lb, lc, ld);
         #pragma omp for schedule(dynamic, 1)
         for (int64_t w = 0; w < (int64_t)nwork; w++) {
             uint32_t ik = rows ? rows[w] : (uint32_t)w;

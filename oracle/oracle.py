@@ -148,10 +148,10 @@ def eri_shell_quartet_grad(la, lb, lc, ld, center, ai, A, aj, B, ak, C, al, D, o
 def _prim_tables(prim_info, prim_count, prim_aoinds=None):
     """prim_info: dict l -> array (5, count); returns ctypes arrays and keep-alive list."""
     keep = []
-    infos = (_f64p * 3)()
-    aoinds = (_u32p * 3)()
-    counts = np.zeros(3, dtype=np.uint32)
-    for l in range(3):
+    infos = (_f64p * 4)()
+    aoinds = (_u32p * 4)()
+    counts = np.zeros(4, dtype=np.uint32)
+    for l in range(4):
         if l in prim_info and prim_info[l] is not None:
             a, p = _f(prim_info[l])
             keep.append(a)

@@ -38,7 +38,7 @@ def oracle_K(rl: ReferenceLists, cls: str, omega=0.0, rows=None):
 
 
 def oracle_jk_all(rl: ReferenceLists, omega=0.0):
-    from vlxb.lists import j_classes, k_classes
+    from vlxb.lists import j_classes_all as j_classes, k_classes_all as k_classes
 
     matJ = {k: np.zeros(len(v.first)) for k, v in rl.jlists.items()}
     matK = {k: np.zeros(len(v.pair_i)) for k, v in rl.kpairs.items()}

@@ -20,7 +20,10 @@ def test_header_lists_all_reference_classes():
     names = declared()
     j = [n for n in names if n.startswith("vlxb_computeCoulombFock") and not n.endswith("_noalloc")]
     k = [n for n in names if n.startswith("vlxb_computeExchangeFock")]
-    assert len(j) == 36 and len(k) == 54
+    # the reference's 36 + 54 s/p/d classes, plus 64 + 106 with f shells
+    assert len([n for n in j if "F" not in n[len("vlxb_computeCoulombFock"):]]) == 36
+    assert len([n for n in k if "F" not in n[len("vlxb_computeExchangeFock"):]]) == 54
+    assert len(j) == 36 + 64 and len(k) == 54 + 106
     assert [n for n in names if n.endswith("_noalloc")] == ["vlxb_computeCoulombFockSSSS_noalloc"]
     assert "vlxb_computeCoulombFockDDDD" in j and "vlxb_computeExchangeFockSDPD" in k and "vlxb_computeExchangeFockPDSD" not in k
 
@@ -51,6 +54,26 @@ def test_python_binding_matches_header():
     for cls in ABI.k_classes():
         sig = f"int vlxb_computeExchangeFock{cls.upper()}(" + ", ".join(ABI.k_params(cls)) + ");"
         assert sig in hdr
+
+
+def test_f_shell_entry_points_declared_and_bound():
+    """The 64 Coulomb and 106 exchange classes with f shells (this library's
+    own: the reference emits s/p/d only) are declared with the generated
+    entry points' conventions and bound by the Python layer."""
+    from vlxb._lib import ABI, lib
+
+    hdr = open(HDR).read()
+    jf, kf = ABI.jf_classes(), ABI.kf_classes()
+    assert len(jf) == 64 and len(kf) == 106
+    assert all("f" in c for c in jf + kf)
+    for cls in jf:
+        assert f"int vlxb_computeCoulombFock{cls.upper()}(" + ", ".join(ABI.j_params(cls)) + ");" in hdr
+    for cls in kf:
+        assert f"int vlxb_computeExchangeFock{cls.upper()}(" + ", ".join(ABI.k_params(cls)) + ");" in hdr
+    assert ABI.j_params("sfsf")[1:5] == ["const double* s_prim_info", "uint32_t s_prim_count",
+                                         "const double* f_prim_info", "uint32_t f_prim_count"]
+    L = lib()
+    assert set(jf) <= set(L.j_params) and set(kf) <= set(L.k_params)
 
 
 def test_gradient_entry_points_declared_and_bound():

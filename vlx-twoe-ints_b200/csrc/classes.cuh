@@ -15,8 +15,8 @@ namespace vlxb {
 
 struct CoulombArgs {
     double* mat_J;
-    const double* info[3];  // prim_info by angular momentum (s, p, d)
-    uint32_t count[3];      // prim_count by angular momentum
+    const double* info[4];  // prim_info by angular momentum (s, p, d, f)
+    uint32_t count[4];      // prim_count by angular momentum
     const double* cd_D;
     const double* ab_Q;
     const double* cd_Q;
@@ -42,9 +42,9 @@ struct ExchangeArgs {
     const uint32_t* pair_i;
     const uint32_t* pair_k;
     uint32_t n_ik;
-    const double* info[3];
-    const uint32_t* aoinds[3];
-    uint32_t count[3];
+    const double* info[4];
+    const uint32_t* aoinds[4];
+    uint32_t count[4];
     double maxD;
     const double* D;
     uint32_t naos;
@@ -56,7 +56,7 @@ struct ExchangeArgs {
     double omega;
     double thr;
     // batched calls over several molecules (all null / 0 for a class call):
-    const uint32_t* aoinds_col[3];  // density column index per prim component (default: aoinds)
+    const uint32_t* aoinds_col[4];  // density column index per prim component (default: aoinds)
     uint32_t D_stride;              // row stride of D (default: naos)
     uint32_t key_naos;              // bound on the AO indices in aoinds (default: naos)
     const int32_t* prim_mol_a;      // molecule of every type-a primitive

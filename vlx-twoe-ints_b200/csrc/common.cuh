@@ -25,7 +25,7 @@ constexpr double BOYS_H = 0.05;
 constexpr double BOYS_INV_H = 20.0;
 constexpr double BOYS_TMAX = 36.0;
 constexpr int BOYS_NGRID = 721;  // BOYS_TMAX / BOYS_H + 1
-constexpr int BOYS_NCOL = 18;    // max m needed: 8 + BOYS_NT - 1 = 15, padded
+constexpr int BOYS_NCOL = 20;    // max m needed: 12 (f shells) + BOYS_NT - 1 = 19
 constexpr int MAX_L = 8;
 
 constexpr double PI_D = 3.141592653589793238462643383279502884;

@@ -24,29 +24,40 @@ from __future__ import annotations
 import os
 import sys
 
-ANG = "spd"
-LV = {"s": 0, "p": 1, "d": 2}
+ANG = "spd"     # the classes the reference emits (the drop-in set)
+ANG_F = "spdf"  # with the f classes, this library's own entry points
+LV = {"s": 0, "p": 1, "d": 2, "f": 3}
 
 
-def j_classes():
-    pairs = [a + b for i, a in enumerate(ANG) for b in ANG[i:]]
+def j_classes(ang=ANG):
+    pairs = [a + b for i, a in enumerate(ang) for b in ang[i:]]
     return [ab + cd for ab in pairs for cd in pairs]
 
 
-def k_classes():
+def k_classes(ang=ANG):
     out = []
-    for i, a in enumerate(ANG):
-        for c in ANG[i:]:
-            for b in ANG:
-                for d in ANG:
+    for i, a in enumerate(ang):
+        for c in ang[i:]:
+            for b in ang:
+                for d in ang:
                     out.append(a + b + c + d)
     return out
+
+
+def jf_classes():
+    """Coulomb classes with at least one f shell (64)."""
+    return [c for c in j_classes(ANG_F) if "f" in c]
+
+
+def kf_classes():
+    """Exchange classes with at least one f shell (106)."""
+    return [c for c in k_classes(ANG_F) if "f" in c]
 
 
 def j_params(cls):
     a, b, c, d = cls
     p = ["double* mat_J"]
-    for x in ANG:
+    for x in ANG_F:
         if x in cls:
             p += [f"const double* {x}_prim_info", f"uint32_t {x}_prim_count"]
     p += [f"const double* {c}{d}_mat_D", f"const double* {a}{b}_mat_Q_local", f"const double* {c}{d}_mat_Q",
@@ -70,7 +81,7 @@ def k_params(cls):
     same = (c + d) == (a + b)
     p = ["double* mat_K", f"const uint32_t* pair_inds_i_for_K_{a}{c}", f"const uint32_t* pair_inds_k_for_K_{a}{c}",
          f"uint32_t pair_inds_count_for_K_{a}{c}"]
-    for x in ANG:
+    for x in ANG_F:
         if x in cls:
             p += [f"const double* {x}_prim_info", f"const uint32_t* {x}_prim_aoinds", f"uint32_t {x}_prim_count"]
     p += [f"double {b}{d}_max_D", "const double* mat_D_full_AO", "uint32_t naos"]
@@ -134,7 +145,7 @@ def header():
          "/* ABI version (major * 10000 + minor * 100 + patch).  No reference counterpart. */",
          "int vlxb_version(void);", "",
          "/* Schwarz helper for callers that build the lists: for n primitive shell",
-         "   pairs (P[t] of type la, Q[t] of type lb, la <= lb <= 2) writes",
+         "   pairs (P[t] of type la, Q[t] of type lb, la <= lb <= 3) writes",
          "   out[t] = max over components of sqrt|(ab|ab)| / |S_ab|, S_ab the pair",
          "   prefactor.  The reference's caller computes its Q_ij outside the",
          "   generator (inputs ab_mat_Q_local, Q_K_ab of gen_coulomb.py:81,",
@@ -351,6 +362,20 @@ def header():
         L.append(f"/* replaces computeExchangeFock{cls.upper()} (gen_exchange.py:75-115; "
                  "class list new_exchange_code/gen_eri_exchange.py:39-56) */")
         L.append(f"int vlxb_computeExchangeFock{cls.upper()}(" + ", ".join(k_params(cls)) + ");")
+    L += ["", "/* ---- f shells: this library's own entry points ----",
+          "   The reference's writer emits s, p and d classes only (eriwriter.py:44-62),",
+          "   although its ERI engine takes any number of Cartesian indices (eri.py:59).",
+          "   These entry points extend the scheme to f with the same argument",
+          "   conventions, f components ordered like d (x^3 first, then by decreasing",
+          "   y power: xxx xxy xxz xyy xyz xzz yyy yyz yzz zzz).  One generic kernel per",
+          "   kind evaluates them component quartet by component quartet (runtime",
+          "   angular momenta, McMurchie-Davidson form); FP64 whatever the",
+          "   mixed-precision cutoff; not counted by vlxb_quartetCounters; no",
+          "   gradient or batched entry points.  No reference counterpart. */"]
+    for cls in jf_classes():
+        L.append(f"int vlxb_computeCoulombFock{cls.upper()}(" + ", ".join(j_params(cls)) + ");")
+    for cls in kf_classes():
+        L.append(f"int vlxb_computeExchangeFock{cls.upper()}(" + ", ".join(k_params(cls)) + ");")
     L += ["", "#ifdef __cplusplus", "}", "#endif", "", "#endif /* VLXB_H */", ""]
     return "\n".join(L)
 
@@ -368,7 +393,51 @@ def abi_cu():
     for cls in k_classes():
         L.append(f"int exchange_{cls}(const ExchangeArgs&, cudaStream_t);")
         L.append(f"int exchange_grad_{cls}(const ExchangeArgs&, int64_t, cudaStream_t);")
+    L.append("int run_coulomb_f(int la, int lb, int lc, int ld, const CoulombArgs&, cudaStream_t);")
+    L.append("int run_exchange_f(int la, int lb, int lc, int ld, const ExchangeArgs&, cudaStream_t);")
     L += ["}  // namespace vlxb", "", 'extern "C" {', ""]
+    for cls in jf_classes():
+        a, b, c, d = cls
+        la, lb, lc, ld = (LV[x] for x in cls)
+        L.append(f"int vlxb_computeCoulombFock{cls.upper()}(" + ", ".join(j_params(cls)) + ")")
+        L.append("{")
+        L.append("    (void)boys_func_table; (void)boys_func_ft;")
+        L.append("    vlxb::CoulombArgs A{};")
+        L.append("    A.mat_J = mat_J;")
+        for x in ANG_F:
+            if x in cls:
+                L.append(f"    A.info[{LV[x]}] = {x}_prim_info; A.count[{LV[x]}] = {x}_prim_count;")
+        L += [f"    A.cd_D = {c}{d}_mat_D; A.ab_Q = {a}{b}_mat_Q_local; A.cd_Q = {c}{d}_mat_Q;",
+              f"    A.ab_first = {a}{b}_first_inds_local; A.ab_second = {a}{b}_second_inds_local;",
+              f"    A.ab_pdata = {a}{b}_pair_data_local; A.n_ab = {a}{b}_prim_pair_count_local;",
+              f"    A.cd_first = {c}{d}_first_inds; A.cd_second = {c}{d}_second_inds;",
+              f"    A.cd_pdata = {c}{d}_pair_data; A.n_cd = {c}{d}_prim_pair_count;",
+              "    A.thr = eri_threshold;",
+              f"    return vlxb::run_coulomb_f({la}, {lb}, {lc}, {ld}, A, (cudaStream_t)stream);", "}", ""]
+    for cls in kf_classes():
+        a, b, c, d = cls
+        la, lb, lc, ld = (LV[x] for x in cls)
+        same = (c + d) == (a + b)
+        L.append(f"int vlxb_computeExchangeFock{cls.upper()}(" + ", ".join(k_params(cls)) + ")")
+        L.append("{")
+        L.append("    (void)boys_func_table; (void)boys_func_ft;")
+        L.append("    vlxb::ExchangeArgs A{};")
+        L.append(f"    A.mat_K = mat_K; A.pair_i = pair_inds_i_for_K_{a}{c}; A.pair_k = pair_inds_k_for_K_{a}{c};")
+        L.append(f"    A.n_ik = pair_inds_count_for_K_{a}{c};")
+        for x in ANG_F:
+            if x in cls:
+                L.append(f"    A.info[{LV[x]}] = {x}_prim_info; A.aoinds[{LV[x]}] = {x}_prim_aoinds; "
+                         f"A.count[{LV[x]}] = {x}_prim_count;")
+        L.append(f"    A.maxD = {b}{d}_max_D; A.D = mat_D_full_AO; A.naos = naos;")
+        cd = f"{a}{b}" if same else f"{c}{d}"
+        L.append(f"    A.Q_ab = Q_K_{a}{b}; A.Q_cd = Q_K_{cd};")
+        L.append(f"    A.Dinds_ab = D_inds_K_{a}{b}; A.Dinds_cd = D_inds_K_{cd};")
+        L.append(f"    A.displs_ab = pair_displs_K_{a}{b}; A.displs_cd = pair_displs_K_{cd};")
+        L.append(f"    A.counts_ab = pair_counts_K_{a}{b}; A.counts_cd = pair_counts_K_{cd};")
+        L.append(f"    A.pdata_ab = pair_data_K_{a}{b}; A.pdata_cd = pair_data_K_{cd};")
+        L.append("    A.omega = omega; A.thr = eri_threshold;")
+        L.append(f"    return vlxb::run_exchange_f({la}, {lb}, {lc}, {ld}, A, (cudaStream_t)stream);")
+        L += ["}", ""]
     for cls in j_classes():
         a, b, c, d = cls
         ps = j_params(cls)

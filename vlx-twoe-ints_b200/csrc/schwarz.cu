@@ -14,6 +14,9 @@
 
 namespace vlxb {
 
+int run_schwarz_f(int la, int lb, const double* info_a, uint32_t cnt_a, const double* info_b, uint32_t cnt_b,
+                  const uint32_t* P, const uint32_t* Q, uint32_t n, double* out, cudaStream_t st);
+
 template <int LA, int LB>
 __global__ void __launch_bounds__(128)
 schwarz_kernel(const double* __restrict__ info_a, uint32_t cnt_a, const double* __restrict__ info_b, uint32_t cnt_b,
@@ -53,9 +56,10 @@ extern "C" int vlxb_schwarzBareMax(int la, int lb, const double* info_a, uint32_
 {
     using namespace vlxb;
     if (n == 0) return VLXB_OK;
-    if (!info_a || !info_b || !P || !Q || !out || la < 0 || lb < la || lb > 2) return VLXB_EINVAL;
+    if (!info_a || !info_b || !P || !Q || !out || la < 0 || lb < la || lb > 3) return VLXB_EINVAL;
     int rc = ensure_pool_configured();
     if (rc) return rc;
+    if (lb == 3) return run_schwarz_f(la, lb, info_a, cnt_a, info_b, cnt_b, P, Q, n, out, (cudaStream_t)stream);
     const double* tab = boys_table_device();
     if (!tab) return VLXB_ECUDA;
     cudaStream_t st = (cudaStream_t)stream;

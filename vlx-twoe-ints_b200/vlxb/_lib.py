@@ -53,8 +53,10 @@ class Lib:
         self.cdll = ctypes.CDLL(path)
         self.j_params = {}
         self.k_params = {}
-        for cls in ABI.j_classes():
+        for cls in ABI.j_classes() + ABI.jf_classes():
             ps = ABI.j_params(cls)
+            if "f" in cls and not hasattr(self.cdll, f"vlxb_computeCoulombFock{cls.upper()}"):
+                continue  # a library built without the f classes: calling one raises KeyError
             f = getattr(self.cdll, f"vlxb_computeCoulombFock{cls.upper()}")
             f.argtypes = [_ctype(p) for p in ps]
             f.restype = ctypes.c_int
@@ -73,8 +75,10 @@ class Lib:
             f.argtypes = [_ctype(p) for p in ps]
             f.restype = ctypes.c_int
             self.kg_params[cls] = [ABI.pname(p) for p in ps]
-        for cls in ABI.k_classes():
+        for cls in ABI.k_classes() + ABI.kf_classes():
             ps = ABI.k_params(cls)
+            if "f" in cls and not hasattr(self.cdll, f"vlxb_computeExchangeFock{cls.upper()}"):
+                continue
             f = getattr(self.cdll, f"vlxb_computeExchangeFock{cls.upper()}")
             f.argtypes = [_ctype(p) for p in ps]
             f.restype = ctypes.c_int

@@ -12,7 +12,7 @@ of the benchmark configurations:
     (even-tempered, distinct for every primitive of the atom);
   * contraction coefficients drawn U(0.2, 1) (seeded), then the contracted
     function is normalised;
-  * Cartesian d shells; every component of a shell shares the normalisation
+  * Cartesian d (and f) shells; every component of a shell shares the normalisation
     of its x^l component (so d_xx is unit-normalised, d_xy is not);
   * density D = C C^T with C ~ N(0,1)^(nao x nocc), orthonormalised in the
     overlap metric: C <- C (C^T S C)^(-1/2).
@@ -24,10 +24,14 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+# Cartesian components in the reference's order (x^l first, then by
+# decreasing y power); f follows the same rule.
 CART = {0: [(0, 0, 0)],
         1: [(1, 0, 0), (0, 1, 0), (0, 0, 1)],
-        2: [(2, 0, 0), (1, 1, 0), (1, 0, 1), (0, 2, 0), (0, 1, 1), (0, 0, 2)]}
-NCART = {0: 1, 1: 3, 2: 6}
+        2: [(2, 0, 0), (1, 1, 0), (1, 0, 1), (0, 2, 0), (0, 1, 1), (0, 0, 2)],
+        3: [(3, 0, 0), (2, 1, 0), (2, 0, 1), (1, 2, 0), (1, 1, 1), (1, 0, 2), (0, 3, 0), (0, 2, 1), (0, 1, 2),
+            (0, 0, 3)]}
+NCART = {0: 1, 1: 3, 2: 6, 3: 10}
 
 
 def _dfact(n: int) -> float:

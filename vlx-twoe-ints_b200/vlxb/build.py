@@ -41,7 +41,7 @@ def _run_generators():
 def _sources():
     srcs = [os.path.join(CSRC, "prep.cu"), os.path.join(CSRC, "api.cu"), os.path.join(CSRC, "schwarz.cu"),
             os.path.join(CSRC, "noalloc.cu"), os.path.join(CSRC, "aomap.cu"),
-            os.path.join(CSRC, "listbuild.cu"), os.path.join(GEN, "abi.cu")]
+            os.path.join(CSRC, "listbuild.cu"), os.path.join(CSRC, "fshell.cu"), os.path.join(GEN, "abi.cu")]
     srcs += sorted(glob.glob(os.path.join(GEN, "cls_*.cu")))
     return srcs
 

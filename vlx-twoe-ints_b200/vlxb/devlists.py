@@ -23,7 +23,7 @@ import torch
 from . import lists
 from ._lib import lib
 from .fock import DeviceLists
-from .lists import ANG, LV, NCART
+from .lists import ANG, LMAX, LV, NCART
 
 
 def _u32(t: torch.Tensor) -> torch.Tensor:
@@ -89,7 +89,7 @@ def build_device_lists(mol, D_AO, threshold: float, device="cuda") -> DeviceList
     dl = DeviceLists(device=dev, naos=mol.naos, threshold=threshold, count=dict(pd.count))
     D = D_AO if isinstance(D_AO, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(D_AO))
     dl.D_AO = D.to(dev, dtype=torch.float64).contiguous()
-    ls = [l for l in range(3) if pd.count[l] > 0]
+    ls = [l for l in range(LMAX + 1) if pd.count[l] > 0]
     for l in ls:
         dl.info[l] = torch.from_numpy(np.ascontiguousarray(pd.info[l])).to(dev)
         dl.aoinds[l] = torch.from_numpy(pd.aoinds[l].astype(np.int32)).to(dev)

@@ -14,7 +14,7 @@ import numpy as np
 import torch
 
 from ._lib import lib
-from .lists import ANG, LV, ReferenceLists, j_classes, k_classes
+from .lists import ANG, LMAX, LV, ReferenceLists, j_classes_all, k_classes_all
 
 
 def _i32(a: np.ndarray) -> np.ndarray:
@@ -48,7 +48,7 @@ class DeviceLists:
 def host_arrays(rl: ReferenceLists) -> dict:
     """Flat dict name -> contiguous numpy array (uint32 viewed as int32)."""
     out = {"D_AO": np.ascontiguousarray(rl.D_AO, dtype=np.float64)}
-    for l in range(3):
+    for l in range(LMAX + 1):
         if rl.pd.count[l] > 0:
             out[f"info{l}"] = np.ascontiguousarray(rl.pd.info[l])
             out[f"aoinds{l}"] = _i32(rl.pd.aoinds[l])
@@ -81,7 +81,7 @@ def upload(rl: ReferenceLists, tensors: dict, device, non_blocking: bool = False
     g = {k: v.to(dev, non_blocking=non_blocking) for k, v in tensors.items()}
     dl = DeviceLists(device=dev, naos=rl.naos, threshold=rl.threshold, count=dict(rl.pd.count), maxD=dict(rl.maxD))
     dl.D_AO = g["D_AO"]
-    for l in range(3):
+    for l in range(LMAX + 1):
         if f"info{l}" in g:
             dl.info[l] = g[f"info{l}"]
             dl.aoinds[l] = g[f"aoinds{l}"]
@@ -165,11 +165,11 @@ def build_jk(dl: DeviceLists, stream: torch.cuda.Stream | None = None, omega: fl
         matJ, matK = alloc_outputs(dl)
     with torch.cuda.stream(stream):
         if do_j:
-            for cls in (j_only or j_classes()):
+            for cls in (j_only or j_classes_all()):
                 if cls[:2] in dl.j and cls[2:] in dl.j:
                     L.coulomb(cls, coulomb_args(dl, cls, matJ[cls[:2]], s))
         if do_k:
-            for cls in (k_only or k_classes()):
+            for cls in (k_only or k_classes_all()):
                 ac = cls[0] + cls[2]
                 if ac in dl.kpair and cls[:2] in dl.kpart and cls[2:] in dl.kpart:
                     L.exchange(cls, exchange_args(dl, cls, matK[ac], s, omega))

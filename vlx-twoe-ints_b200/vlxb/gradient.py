@@ -86,6 +86,8 @@ class GradientMap:
     the diagonal flags of same-type lists."""
 
     def __init__(self, lists: dict, fields, atoms: dict, natoms: int, device):
+        if any("f" in k for k in lists):
+            raise ValueError("the nuclear-gradient entry points cover s, p and d shells only")
         self.device = torch.device(device)
         self.natoms = int(natoms)
         self.keys = sorted(lists)

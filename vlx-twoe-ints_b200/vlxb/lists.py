@@ -29,8 +29,10 @@ import numpy as np
 
 from .basis import NCART, Molecule
 
-ANG = "spd"
-LV = {"s": 0, "p": 1, "d": 2}
+ANG = "spdf"   # letters by angular momentum (s, p, d and f)
+SPD = "spd"    # the classes the reference emits
+LV = {"s": 0, "p": 1, "d": 2, "f": 3}
+LMAX = 3
 
 
 @dataclass
@@ -42,13 +44,13 @@ class PrimData:
 
 
 def prim_data(mol: Molecule) -> PrimData:
-    rows = {l: [] for l in range(3)}
+    rows = {l: [] for l in range(LMAX + 1)}
     for sh in mol.shells:
         R = mol.coords[sh.atom]
         for e, c in zip(sh.exps, sh.coefs):
             rows[sh.l].append((e, c, R[0], R[1], R[2], sh.ao0, sh.atom))
     info, aoinds, count, atom = {}, {}, {}, {}
-    for l in range(3):
+    for l in range(LMAX + 1):
         r = rows[l]
         n = len(r)
         inf = np.zeros((5, max(n, 0)))
@@ -150,7 +152,7 @@ def _expand(sp: ShellPairs, keep: np.ndarray, upper: bool):
 def build_lists(mol: Molecule, D_AO: np.ndarray, threshold: float, schwarz_fn) -> ReferenceLists:
     pd = prim_data(mol)
     rl = ReferenceLists(pd=pd, naos=mol.naos, D_AO=np.ascontiguousarray(D_AO), threshold=threshold)
-    ls = [l for l in range(3) if pd.count[l] > 0]
+    ls = [l for l in range(LMAX + 1) if pd.count[l] > 0]
     for la in ls:
         for lb in ls:
             if la <= lb:
@@ -261,10 +263,23 @@ def energy(D: np.ndarray, J: np.ndarray, K: np.ndarray) -> float:
     return float(np.sum(D * (J - 0.5 * K)))
 
 
-def j_classes():
-    pairs = [a + b for i, a in enumerate(ANG) for b in ANG[i:]]
+def j_classes(ang: str = SPD):
+    """Coulomb classes (ab|cd), a <= b and c <= d in angular momentum; the
+    reference's 36 s/p/d classes by default."""
+    pairs = [a + b for i, a in enumerate(ang) for b in ang[i:]]
     return [ab + cd for ab in pairs for cd in pairs]
 
 
-def k_classes():
-    return [a + b + c + d for i, a in enumerate(ANG) for c in ANG[i:] for b in ANG for d in ANG]
+def k_classes(ang: str = SPD):
+    """Exchange classes (ab|cd), a <= c; the reference's 54 by default."""
+    return [a + b + c + d for i, a in enumerate(ang) for c in ang[i:] for b in ang for d in ang]
+
+
+def j_classes_all():
+    """The 100 Coulomb classes of s, p, d and f shells."""
+    return j_classes(ANG)
+
+
+def k_classes_all():
+    """The 160 exchange classes of s, p, d and f shells."""
+    return k_classes(ANG)
