@@ -904,8 +904,17 @@ def run_ours(args):
     total_flops = sum(r[4] for r in per_class)
     total_t = sum(r[2] for r in per_class)
     ach_dom = dom[4] / dom[2] / 1e12
+    # DRAM bytes of the dominant launch from one ncu capture of this workload
+    # (profiles/exchange_col_kernel_pddd_40atom_traffic.md), when the
+    # dominant class is the captured one
+    traffic = None
+    tpath = os.path.join(PKG, "vlxb", "traffic_b200.json")
+    if os.path.exists(tpath):
+        tr = json.load(open(tpath))
+        if dom[0] == "K" and dom[1] == "pddd" and args.config == "medium":
+            traffic = tr["dram_bytes_read"] + tr["dram_bytes_write"]
     roofline = {"bound": "fp64", "achieved": ach_dom, "peak": peak, "unit": "TFLOP/s", "frac": ach_dom / peak,
-                "traffic": None,
+                "traffic": traffic, "traffic_unit": "bytes per launch (DRAM read + write, one ncu capture)",
                 "kernel": f"{dom[0]} class {dom[1].upper()} (prep + integral kernel)",
                 "build_achieved": total_flops / total_t / 1e12, "build_frac": total_flops / total_t / 1e12 / peak,
                 "peak_source": "measured: FP64 FMA probe kernel on this GPU (MEASURED_PEAKS.json has no FP64 figure)"}

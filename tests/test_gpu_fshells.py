@@ -68,6 +68,26 @@ def test_spdf_every_class_vs_oracle(spdf):
     assert abs(lists.energy(wl.D, J, K) - lists.energy(wl.D, Jo, Ko)) < 1e-10
 
 
+def test_spdf_device_built_lists(spdf):
+    """The device list builder with f shells (pair data and Schwarz values of
+    f pairs on the GPU): the same J / K as the host-built lists."""
+    from vlxb import devlists
+
+    wl, rl = spdf
+    dl_h = fock.to_device(rl)
+    dl_d = devlists.build_device_lists(wl.mol, wl.D, wl.threshold)
+    Jh, Kh = fock.build_jk(dl_h)
+    Jd, Kd = fock.build_jk(dl_d)
+    torch.cuda.synchronize()
+    host_d = devlists.to_host(dl_d, wl.mol)
+    a = lists.contract_J(rl, {k: v.cpu().numpy() for k, v in Jh.items()})
+    b = lists.contract_J(host_d, {k: v.cpu().numpy() for k, v in Jd.items()})
+    assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max()
+    a = lists.contract_K(rl, {k: v.cpu().numpy() for k, v in Kh.items()})
+    b = lists.contract_K(host_d, {k: v.cpu().numpy() for k, v in Kd.items()})
+    assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max()
+
+
 def test_spdf_range_separated_exchange(spdf):
     wl, rl = spdf
     dl = fock.to_device(rl)

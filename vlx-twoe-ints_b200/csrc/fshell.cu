@@ -299,6 +299,53 @@ schwarz_fshell_kernel(int la, int lb, const double* __restrict__ info_a, uint32_
     }
 }
 
+// Pair prefactor S_PQ = c_P c_Q (pi / p)^(3/2) exp(-a b / p |A - B|^2) and
+// Q_PQ = |S_PQ| sqrt(max bare diagonal) of pairs with an f shell
+// (vlxb_shellPairData).
+__global__ void __launch_bounds__(FS_THREADS)
+shell_pair_fshell_kernel(int la, int lb, const double* __restrict__ info_a, uint32_t cnt_a,
+                         const double* __restrict__ info_b, uint32_t cnt_b, const uint32_t* __restrict__ P,
+                         const uint32_t* __restrict__ Q, uint32_t n, double* __restrict__ S_out,
+                         double* __restrict__ q_out, const double* __restrict__ tab)
+{
+    const int na = ncart(la), nb = ncart(lb);
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const uint32_t i = P[t], j = Q[t];
+        const FPrim A0 = fprim(info_a, cnt_a, la, i * (uint32_t)na);
+        const FPrim B0 = fprim(info_b, cnt_b, lb, j * (uint32_t)nb);
+        const double p = A0.alpha + B0.alpha, iz = 1.0 / p;
+        double R2 = 0.0;
+        for (int x = 0; x < 3; x++) R2 += (A0.r[x] - B0.r[x]) * (A0.r[x] - B0.r[x]);
+        const double pi_p = 3.14159265358979323846 * iz;
+        const double S = __ldg(info_a + i + (int64_t)cnt_a) * __ldg(info_b + j + (int64_t)cnt_b) * pi_p *
+                         sqrt(pi_p) * exp(-A0.alpha * B0.alpha * iz * R2);
+        double m = 0.0;
+        for (int ca = 0; ca < na; ca++)
+            for (int cb = 0; cb < nb; cb++) {
+                const FPrim A = fprim(info_a, cnt_a, la, i * (uint32_t)na + ca);
+                const FPrim B = fprim(info_b, cnt_b, lb, j * (uint32_t)nb + cb);
+                m = fmax(m, fabs(eri_component(A, B, A, B, 0.0, tab)));
+            }
+        S_out[t] = S;
+        q_out[t] = fabs(S) * sqrt(m);
+    }
+}
+
+int run_shell_pair_f(int la, int lb, const double* info_a, uint32_t cnt_a, const double* info_b, uint32_t cnt_b,
+                     const uint32_t* P, const uint32_t* Q, uint32_t n, double* S_out, double* q_out,
+                     cudaStream_t st)
+{
+    const double* tab = boys_table_device();
+    if (!tab) return VLXB_ECUDA;
+    const uint32_t want = (n + FS_THREADS - 1) / FS_THREADS;
+    const int grid = (int)(want < 148u * 64u ? want : 148u * 64u);
+    shell_pair_fshell_kernel<<<grid, FS_THREADS, 0, st>>>(la, lb, info_a, cnt_a, info_b, cnt_b, P, Q, n, S_out, q_out,
+                                                          tab);
+    note_launches();
+    VLXB_CHECK_CUDA(cudaGetLastError());
+    return VLXB_OK;
+}
+
 int run_schwarz_f(int la, int lb, const double* info_a, uint32_t cnt_a, const double* info_b, uint32_t cnt_b,
                   const uint32_t* P, const uint32_t* Q, uint32_t n, double* out, cudaStream_t st)
 {

@@ -229,7 +229,7 @@ def header():
          "   gen_coulomb.py:80-90 and gen_exchange.py:78-110).  No reference",
          "   counterpart.",
          "   vlxb_shellPairData: for n primitive shell pairs (P[t] of type la, Q[t]",
-         "   of type lb, la <= lb <= 2) S_out[t] = c_P c_Q (pi/p)^(3/2)",
+         "   of type lb, la <= lb <= 3) S_out[t] = c_P c_Q (pi/p)^(3/2)",
          "   exp(-ab/p |A-B|^2) and q_out[t] = |S_out[t]| * max over components",
          "   sqrt|(ab|ab)| / |S_ab| (the Schwarz value of every component pair).",
          "   vlxb_gatherPairDensity: out[t] = D_AO[ao_a(first[t])][ao_b(second[t])]",

@@ -21,6 +21,10 @@
 
 namespace vlxb {
 
+int run_shell_pair_f(int la, int lb, const double* info_a, uint32_t cnt_a, const double* info_b, uint32_t cnt_b,
+                     const uint32_t* P, const uint32_t* Q, uint32_t n, double* S_out, double* q_out,
+                     cudaStream_t st);
+
 // S_PQ = c_P c_Q (pi / p)^(3/2) exp(-a b / p |A - B|^2) and
 // Q_PQ = |S_PQ| * max over components sqrt|(ab|ab)| / |S_ab| (the bare
 // diagonal integral of the pair, as vlxb_schwarzBareMax).
@@ -102,12 +106,13 @@ extern "C" int vlxb_shellPairData(int la, int lb, const double* info_a, uint32_t
 {
     using namespace vlxb;
     if (n == 0) return VLXB_OK;
-    if (!info_a || !info_b || !P || !Q || !S_out || !q_out || la < 0 || lb < la || lb > 2) return VLXB_EINVAL;
+    if (!info_a || !info_b || !P || !Q || !S_out || !q_out || la < 0 || lb < la || lb > 3) return VLXB_EINVAL;
     int rc = ensure_pool_configured();
     if (rc) return rc;
     const double* tab = boys_table_device();
     if (!tab) return VLXB_ECUDA;
     cudaStream_t st = (cudaStream_t)stream;
+    if (lb == 3) return run_shell_pair_f(la, lb, info_a, cnt_a, info_b, cnt_b, P, Q, n, S_out, q_out, st);
     const int grid = (int)((n + 127) / 128 < 148 * 64 ? (n + 127) / 128 : 148 * 64);
 #define VLXB_SPD(A, B)                                                                                        \
     if (la == A && lb == B)                                                                                   \
