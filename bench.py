@@ -27,7 +27,8 @@ After the timed steps the same line carries the other legs (all on this GPU):
            cores (reference expressions), every value checked
   large    the large sparse recipe (25 bohr^3 per atom, 4s3p2d) at 48 atoms
            (1200 AOs; --large-atoms 200 runs the 5000-AO cluster, whose
-           incremental build is about 6.4e12 quartets): incremental build on
+           incremental build is 6.409e12 quartets, about 48 min of one B200
+           in mixed precision): incremental build on
            dD of norm 1e-3, density-weighted screening at 1e-11, mixed
            precision with FP64 accumulation
   batched / served   the batching and serving patterns (served: one rate
@@ -96,7 +97,7 @@ def parse():
     ap.add_argument("--small-steps", type=int, default=5, help="5-atom leg: timed builds (0 skips the leg)")
     ap.add_argument("--large-atoms", type=int, default=48,
                     help="large sparse leg: atoms at 25 bohr^3/atom (0 skips the leg; 200 is the full cluster, "
-                         "about 6.4e12 quartets per incremental build)")
+                         "6.4e12 quartets per incremental build, ~48 min)")
     ap.add_argument("--pattern-fp32-cut", type=float, default=1e-6,
                     help="batched / served legs: FP32 below this bound, inside the FP32 error budget")
     ap.add_argument("--large-no-fp64", action="store_true",
@@ -905,13 +906,13 @@ def run_ours(args):
     total_t = sum(r[2] for r in per_class)
     ach_dom = dom[4] / dom[2] / 1e12
     # DRAM bytes of the dominant launch from one ncu capture of this workload
-    # (profiles/exchange_col_kernel_pddd_40atom_traffic.md), when the
-    # dominant class is the captured one
+    # (profiles/*_40atom_traffic.md), when the dominant class and its kernel
+    # variant are the captured ones
     traffic = None
     tpath = os.path.join(PKG, "vlxb", "traffic_b200.json")
-    if os.path.exists(tpath):
-        tr = json.load(open(tpath))
-        if dom[0] == "K" and dom[1] == "pddd" and args.config == "medium":
+    if os.path.exists(tpath) and args.config == "medium":
+        tr = json.load(open(tpath)).get(f"{dom[0]} {dom[1]}")
+        if tr and tr.get("variant") == L.get_schedule(dom[0], dom[1]):
             traffic = tr["dram_bytes_read"] + tr["dram_bytes_write"]
     roofline = {"bound": "fp64", "achieved": ach_dom, "peak": peak, "unit": "TFLOP/s", "frac": ach_dom / peak,
                 "traffic": traffic, "traffic_unit": "bytes per launch (DRAM read + write, one ncu capture)",

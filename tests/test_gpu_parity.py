@@ -268,14 +268,10 @@ def _k_variants(cls):
     import os as _o
     _s.path.insert(0, _o.path.join(_o.path.dirname(_o.path.dirname(_o.path.abspath(__file__))),
                                    "vlx-twoe-ints_b200", "csrc"))
-    from gen_column import ColumnPlan, k_smem_bytes
+    from gen_column import k_variants
 
     l = [{"s": 0, "p": 1, "d": 2}[x] for x in cls]
-    out = [0]
-    for ori in (0, 1):
-        if k_smem_bytes(ColumnPlan(*l, ori)) <= 46 * 1024:
-            out += [1 + ori, 3 + ori]
-    return out
+    return k_variants(*l)
 
 
 @pytest.mark.parametrize("variant", [0, 1, 2, 3])
@@ -303,11 +299,12 @@ def test_golden_every_coulomb_variant(golden, variant):
             L.set_schedule("J", c, v)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", list(range(13)))
 def test_golden_every_exchange_variant(golden, variant):
     """All exchange kernels (thread per quartet; column with bra or ket lanes;
-    the same with contracted partners) on every class where the variant is
-    compiled."""
+    the same with contracted partners; packed column plans, also on the
+    pair's second centre, with and without contracted partners) on every
+    class where the variant is compiled."""
     z = golden
     L = lib()
     saved = {c: L.get_schedule("K", c) for c in tf.k_classes()}
@@ -399,7 +396,7 @@ def test_fp32_budget_bounds_the_fp32_work():
     assert 0.0 < diff <= 1e-4 * scale
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 9, 10, 11, 12])
 def test_contracted_exchange_variants_vs_oracle(variant):
     """Degree-3 contracted s/p/d shells (partner groups of up to 3 primitives
     with one S per record): every exchange class through one kernel variant

@@ -34,4 +34,5 @@ def test_compiled_variants():
     assert compiled_variants("J", "ssss") == [0, 1, 2, 3]
     assert 0 not in compiled_variants("J", "dddd")  # its thread kernel spills and is never timed
     kv = compiled_variants("K", "pddd")
-    assert set(kv) <= {0, 1, 2, 3, 4} and {1, 3} <= set(kv)
+    assert set(kv) <= set(range(13)) and {1, 3, 7, 11} <= set(kv) and 0 not in kv
+    assert 5 in compiled_variants("K", "dpdd") and 6 in compiled_variants("K", "dddp")

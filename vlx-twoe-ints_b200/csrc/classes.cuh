@@ -209,6 +209,46 @@ int run_coulomb_grad(const CoulombArgs& a, int64_t gstride, cudaStream_t st)
     return run_coulomb_impl<LA, LB, LC, LD, 1>(a, st, ar, tab, nullptr, fp32_cut_get(), gstride);
 }
 
+// One contracted-partner column exchange launch of plan kind ORI when that
+// plan is built for the class; false otherwise.
+template <int LA, int LB, int LC, int LD, int ORI>
+bool launch_exchange_colc(int pm, int grid, cudaStream_t st, const KOutBlocks& out, const KPartnerRecs& rab,
+                          const KPartnerRecs& rcd, const KGroups& kgab, const KGroups& kgcd, const KDensity& dm,
+                          const ExchangeArgs& a, const BoysTabs& tab, unsigned long long* qk, double cut, double budget)
+{
+    if constexpr (ColTab<LA, LB, LC, LD, ORI>::K_FITS) {
+        if (pm == 0)
+            exchange_colc_kernel<LA, LB, LC, LD, ORI, 0><<<grid, K_THREADS, 0, st>>>(
+                out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
+        else
+            exchange_colc_kernel<LA, LB, LC, LD, ORI, 1><<<grid, K_THREADS, 0, st>>>(
+                out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
+        return true;
+    } else {
+        return false;
+    }
+}
+
+// One column exchange launch of plan kind ORI when that plan is built for the
+// class (its ColTab fits); false otherwise.
+template <int LA, int LB, int LC, int LD, int ORI>
+bool launch_exchange_col(int pm, int grid, cudaStream_t st, const KOutBlocks& out, const KPartnerRecs& rab,
+                         const KPartnerRecs& rcd, const KDensity& dm, const ExchangeArgs& a, const BoysTabs& tab,
+                         unsigned long long* qk, double cut, double budget)
+{
+    if constexpr (ColTab<LA, LB, LC, LD, ORI>::K_FITS) {
+        if (pm == 0)
+            exchange_col_kernel<LA, LB, LC, LD, ORI, 0><<<grid, K_THREADS, 0, st>>>(
+                out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
+        else
+            exchange_col_kernel<LA, LB, LC, LD, ORI, 1><<<grid, K_THREADS, 0, st>>>(
+                out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
+        return true;
+    } else {
+        return false;
+    }
+}
+
 template <int LA, int LB, int LC, int LD>
 int run_exchange(const ExchangeArgs& a, cudaStream_t st)
 {
@@ -257,7 +297,7 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
     const double budget = cut > 0.0 ? fp32_budget_get() : 0.0;
     KGroups kgab{}, kgcd{};
     const uint32_t key_naos = a.key_naos ? a.key_naos : a.naos;
-    if (var == 3 || var == 4) {
+    if (var == 3 || var == 4 || var >= 9) {
         // contracted variants: group partner records by contracted partner shell
         rc = contract_groups(ar, npa, gab, a.aoinds[LB], key_naos);
         if (rc) return rc;
@@ -279,7 +319,7 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
             if (rc) return rc;
         }
     }
-    if (var == 3 || var == 4) {
+    if (var == 3 || var == 4 || var >= 9) {
         kgab = KGroups{gab.gseg, gab.gq, gab.gbeg, gab.gcnt, gab.msp, gab.mq, gab.msu, gab.mmask, gab.gqa, gab.gqpre};
         kgcd = KGroups{gcd.gseg, gcd.gq, gcd.gbeg, gcd.gcnt, gcd.msp, gcd.mq, gcd.msu, gcd.mmask, gcd.gqa, gcd.gqpre};
     }
@@ -301,49 +341,25 @@ int run_exchange(const ExchangeArgs& a, cudaStream_t st)
                       a.D, a.D_stride ? a.D_stride : a.naos};
     for (int pm = 0; pm < (cut > 0.0 ? 2 : 1); pm++) {
         bool launched = false;
-        if constexpr (ColTab<LA, LB, LC, LD, 0>::K_FITS) {
-            if (var == 3) {
-                if (pm == 0)
-                    exchange_colc_kernel<LA, LB, LC, LD, 0, 0><<<grid, K_THREADS, 0, st>>>(
-                        out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
-                else
-                    exchange_colc_kernel<LA, LB, LC, LD, 0, 1><<<grid, K_THREADS, 0, st>>>(
-                        out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
-                launched = true;
-            }
+        // column kernels: variants 1, 2 = plan kinds 0, 1; variants 5..8 = packed kinds 2..5;
+        // contracted-partner column kernels: variants 3, 4 = kinds 0, 1; 9..12 = kinds 2..5
+        switch (var) {
+            case 3: launched = launch_exchange_colc<LA, LB, LC, LD, 0>(pm, grid, st, out, rab, rcd, kgab, kgcd, dm, a, tab, qk, cut, budget); break;
+            case 4: launched = launch_exchange_colc<LA, LB, LC, LD, 1>(pm, grid, st, out, rab, rcd, kgab, kgcd, dm, a, tab, qk, cut, budget); break;
+            case 9: launched = launch_exchange_colc<LA, LB, LC, LD, 2>(pm, grid, st, out, rab, rcd, kgab, kgcd, dm, a, tab, qk, cut, budget); break;
+            case 10: launched = launch_exchange_colc<LA, LB, LC, LD, 3>(pm, grid, st, out, rab, rcd, kgab, kgcd, dm, a, tab, qk, cut, budget); break;
+            case 11: launched = launch_exchange_colc<LA, LB, LC, LD, 4>(pm, grid, st, out, rab, rcd, kgab, kgcd, dm, a, tab, qk, cut, budget); break;
+            case 12: launched = launch_exchange_colc<LA, LB, LC, LD, 5>(pm, grid, st, out, rab, rcd, kgab, kgcd, dm, a, tab, qk, cut, budget); break;
+            default: break;
         }
-        if constexpr (ColTab<LA, LB, LC, LD, 1>::K_FITS) {
-            if (var == 4) {
-                if (pm == 0)
-                    exchange_colc_kernel<LA, LB, LC, LD, 1, 0><<<grid, K_THREADS, 0, st>>>(
-                        out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
-                else
-                    exchange_colc_kernel<LA, LB, LC, LD, 1, 1><<<grid, K_THREADS, 0, st>>>(
-                        out, rab, rcd, kgab, kgcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
-                launched = true;
-            }
-        }
-        if constexpr (ColTab<LA, LB, LC, LD, 0>::K_FITS) {
-            if (var == 1) {
-                if (pm == 0)
-                    exchange_col_kernel<LA, LB, LC, LD, 0, 0><<<grid, K_THREADS, 0, st>>>(
-                        out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
-                else
-                    exchange_col_kernel<LA, LB, LC, LD, 0, 1><<<grid, K_THREADS, 0, st>>>(
-                        out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
-                launched = true;
-            }
-        }
-        if constexpr (ColTab<LA, LB, LC, LD, 1>::K_FITS) {
-            if (var == 2) {
-                if (pm == 0)
-                    exchange_col_kernel<LA, LB, LC, LD, 1, 0><<<grid, K_THREADS, 0, st>>>(
-                        out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
-                else
-                    exchange_col_kernel<LA, LB, LC, LD, 1, 1><<<grid, K_THREADS, 0, st>>>(
-                        out, rab, rcd, dm, a.maxD, a.omega, a.thr, a.mat_K, tab, qk, cut, budget);
-                launched = true;
-            }
+        switch (var) {
+            case 1: launched = launch_exchange_col<LA, LB, LC, LD, 0>(pm, grid, st, out, rab, rcd, dm, a, tab, qk, cut, budget); break;
+            case 2: launched = launch_exchange_col<LA, LB, LC, LD, 1>(pm, grid, st, out, rab, rcd, dm, a, tab, qk, cut, budget); break;
+            case 5: launched = launch_exchange_col<LA, LB, LC, LD, 2>(pm, grid, st, out, rab, rcd, dm, a, tab, qk, cut, budget); break;
+            case 6: launched = launch_exchange_col<LA, LB, LC, LD, 3>(pm, grid, st, out, rab, rcd, dm, a, tab, qk, cut, budget); break;
+            case 7: launched = launch_exchange_col<LA, LB, LC, LD, 4>(pm, grid, st, out, rab, rcd, dm, a, tab, qk, cut, budget); break;
+            case 8: launched = launch_exchange_col<LA, LB, LC, LD, 5>(pm, grid, st, out, rab, rcd, dm, a, tab, qk, cut, budget); break;
+            default: break;
         }
         if (!launched) {
             if (pm == 0)

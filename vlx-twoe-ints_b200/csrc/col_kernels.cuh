@@ -6,7 +6,13 @@
 // all lanes with one warp shuffle per step for the coupling term (see
 // gen_column.py).  A warp holds ColTab::P such groups.
 //
-// Exchange (ori 0, lanes = bra e; ori 1, lanes = ket f), per quartet:
+// Plan kinds ORI (gen_column.py): bit 0 the orientation (0: lanes = bra e,
+// 1: lanes = ket f); 2, 3 packed plans (lanes for the target levels only,
+// which start at d; two or five quartets per warp); 4, 5 packed plans whose
+// lane-side pair is built on its second centre: PA -> PB = PA + AB and
+// AB -> BA before the VRR (QC, CD likewise), the lane-side HRR gives (b a|
+// and its result is read transposed.
+// Exchange (orientation 0, lanes = bra e; orientation 1, lanes = ket f), per quartet:
 //   VRR (column) -> lane-side HRR per lane into shared memory (ori 0: ket
 //   HRR (e|cd); ori 1: bra HRR (ab|f)) -> __syncwarp -> each lane takes fixed
 //   units of the other side (ori 0: cd pairs; ori 1: ab pairs), applies the
@@ -66,16 +72,42 @@ __device__ __forceinline__ ColLane make_lane(int lig, int gbase)
 template <int LA, int LB, int LC, int LD, int ORI>
 struct KColShape {
     using CT = ColTab<LA, LB, LC, LD, ORI>;
+    static constexpr int O = ORI & 1;      // orientation
+    static constexpr bool SW = ORI >= 4;   // lane-side pair built on its second centre
     static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
     static constexpr int NL = CT::NL, P = CT::P, NXT = CT::NXT, NYT = CT::NYT;
-    // phase-2 units: ori 0 -> cd pairs (accumulate K[a][c(u)]), ori 1 -> ab pairs (K[a(u)][c])
-    static constexpr int N2 = ORI == 0 ? NC * ND : NA * NB;
+    // phase-2 units: orientation 0 -> cd pairs (accumulate K[a][c(u)]), 1 -> ab pairs (K[a(u)][c])
+    static constexpr int N2 = O == 0 ? NC * ND : NA * NB;
     // row length of the shared lane-side HRR results: odd, so that lanes
     // storing one column of U hit distinct banks
     static constexpr int N2P = N2 | 1;
-    static constexpr int NACC = ORI == 0 ? NA : NC;
+    static constexpr int NACC = O == 0 ? NA : NC;
     static constexpr int NPASS = (N2 + NL - 1) / NL;
+    // U (lane-side HRR rows, per quartet) and red (the block's partials, after
+    // its last quartet) share one shared-memory array
+    static constexpr int U_DOUBLES = (K_THREADS / 32) * P * NXT * N2P;
+    static constexpr int RED_DOUBLES = (K_THREADS / 32) * P * N2 * NACC;
+    static constexpr int POOL_DOUBLES = U_DOUBLES > RED_DOUBLES ? U_DOUBLES : RED_DOUBLES;
+    // position of (a, b) / (c, d) in the lane-side HRR result: (b a| / (d c| when swapped
+    __device__ static constexpr int iab(int a, int b) { return SW && O == 0 ? b * NA + a : a * NB + b; }
+    __device__ static constexpr int icd(int c, int d) { return SW && O == 1 ? d * NC + c : c * ND + d; }
 };
+
+// Second-centre plans: the lane-side pair's VRR starts from B (D) and its
+// HRR runs from B to A (D to C).
+template <int ORI, typename T>
+__device__ __forceinline__ void swap_lane_centre(QVT<T>& q)
+{
+    if constexpr (ORI >= 4) {
+        if constexpr ((ORI & 1) == 0) {
+            q.PAx += q.ABx; q.PAy += q.ABy; q.PAz += q.ABz;
+            q.ABx = -q.ABx; q.ABy = -q.ABy; q.ABz = -q.ABz;
+        } else {
+            q.QCx += q.CDx; q.QCy += q.CDy; q.QCz += q.CDz;
+            q.CDx = -q.CDx; q.CDy = -q.CDy; q.CDz = -q.CDz;
+        }
+    }
+}
 
 template <int LA, int LB, int LC, int LD, int ORI, typename T>
 __device__ __forceinline__ void kcol_quartet(bool act, int jr, int lr, const KPartnerRecs& ab,
@@ -94,12 +126,13 @@ __device__ __forceinline__ void kcol_quartet(bool act, int jr, int lr, const KPa
     QVT<T> q;
     T F[L + 1];
     make_quartet_t<L>(bg, kg, omega, tabs.f64, tabs.f32, q, F);
+    swap_lane_centre<ORI>(q);
     T col[NYT];
     col_vrr<LA, LB, LC, LD, ORI, T>(q, F, ln, col);
     // phase 2a: this lane's HRR over the step side, into shared memory
     if (lane_ok && ln.tidx >= 0) {
         T h[N2];
-        if (ORI == 0) hrr_bra_vector<LC, LD, T>(q.CDx, q.CDy, q.CDz, col, h);
+        if (S::O == 0) hrr_bra_vector<LC, LD, T>(q.CDx, q.CDy, q.CDz, col, h);
         else hrr_bra_vector<LA, LB, T>(q.ABx, q.ABy, q.ABz, col, h);
 #pragma unroll
         for (int u = 0; u < N2; u++) U[ln.tidx][u] = (double)h[u];
@@ -118,11 +151,12 @@ __device__ __forceinline__ void kcol_quartet(bool act, int jr, int lr, const KPa
                 T v[NXT];
 #pragma unroll
                 for (int x = 0; x < NXT; x++) v[x] = (T)U[x][u];
-                if (ORI == 0) {
+                if (S::O == 0) {
                     // unit = (c, d): bra HRR, then K[a][c] += sum_b (ab|cd) Sij[ab] Skl[cd] D[b][d]
                     const int dd = u % ND;
                     T I[NA * NB];
-                    hrr_bra_vector<LA, LB, T>(q.ABx, q.ABy, q.ABz, v, I);
+                    if constexpr (S::SW) hrr_bra_vector<LB, LA, T>(q.ABx, q.ABy, q.ABz, v, I);
+                    else hrr_bra_vector<LA, LB, T>(q.ABx, q.ABy, q.ABz, v, I);
                     const double skl =
                         uni ? sul : (((ml >> u) & 1ull) ? __ldg(cd.S + u * cd.sp_stride + spl) : 0.0);
                     const uint32_t lao = __ldg(dm.d_aoinds + lsh + (int64_t)dm.d_count * dd);
@@ -137,7 +171,7 @@ __device__ __forceinline__ void kcol_quartet(bool act, int jr, int lr, const KPa
                         for (int a = 0; a < NA; a++) {
                             T s = (T)0;
 #pragma unroll
-                            for (int b = 0; b < NB; b++) s = fma(I[a * NB + b], wv[b], s);
+                            for (int b = 0; b < NB; b++) s = fma(I[S::iab(a, b)], wv[b], s);
                             Kacc[p][a] += (double)s;
                         }
                     } else {
@@ -148,7 +182,7 @@ __device__ __forceinline__ void kcol_quartet(bool act, int jr, int lr, const KPa
                             for (int b = 0; b < NB; b++) {
                                 const T sij = ((mj >> (a * NB + b)) & 1ull)
                                                   ? (T)__ldg(ab.S + (a * NB + b) * ab.sp_stride + spj) : (T)0;
-                                s = fma(I[a * NB + b] * sij, wv[b], s);
+                                s = fma(I[S::iab(a, b)] * sij, wv[b], s);
                             }
                             Kacc[p][a] += (double)s;
                         }
@@ -157,7 +191,8 @@ __device__ __forceinline__ void kcol_quartet(bool act, int jr, int lr, const KPa
                     // unit = (a, b): ket HRR, then K[a][c] += Sij[ab] sum_d (ab|cd) Skl[cd] D[b][d]
                     const int bb = u % NB;
                     T I[NC * ND];
-                    hrr_bra_vector<LC, LD, T>(q.CDx, q.CDy, q.CDz, v, I);
+                    if constexpr (S::SW) hrr_bra_vector<LD, LC, T>(q.CDx, q.CDy, q.CDz, v, I);
+                    else hrr_bra_vector<LC, LD, T>(q.CDx, q.CDy, q.CDz, v, I);
                     const double sij =
                         uni ? suj : (((mj >> u) & 1ull) ? __ldg(ab.S + u * ab.sp_stride + spj) : 0.0);
                     const uint32_t jao = __ldg(dm.b_aoinds + jsh + (int64_t)dm.b_count * bb);
@@ -172,7 +207,7 @@ __device__ __forceinline__ void kcol_quartet(bool act, int jr, int lr, const KPa
                         for (int c = 0; c < NC; c++) {
                             T s = (T)0;
 #pragma unroll
-                            for (int d = 0; d < ND; d++) s = fma(I[c * ND + d], wv[d], s);
+                            for (int d = 0; d < ND; d++) s = fma(I[S::icd(c, d)], wv[d], s);
                             Kacc[p][c] += (double)s;
                         }
                     } else {
@@ -183,7 +218,7 @@ __device__ __forceinline__ void kcol_quartet(bool act, int jr, int lr, const KPa
                             for (int d = 0; d < ND; d++) {
                                 const T skl = ((ml >> (c * ND + d)) & 1ull)
                                                   ? (T)__ldg(cd.S + (c * ND + d) * cd.sp_stride + spl) : (T)0;
-                                s = fma(I[c * ND + d] * skl, wv[d], s);
+                                s = fma(I[S::icd(c, d)] * skl, wv[d], s);
                             }
                             Kacc[p][c] += (double)s;
                         }
@@ -207,8 +242,9 @@ exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity d
     constexpr int NW = K_THREADS / 32;
     constexpr int NL = S::NL, P = S::P, NXT = S::NXT;
     constexpr int N2 = S::N2, NACC = S::NACC, NPASS = S::NPASS;
-    __shared__ double U[NW][P][NXT][S::N2P];
-    __shared__ double red[NW][P][N2][NACC];
+    __shared__ double pool[S::POOL_DOUBLES];
+    double(*U)[P][NXT][S::N2P] = reinterpret_cast<double(*)[P][NXT][S::N2P]>(pool);
+    double(*red)[P][N2][NACC] = reinterpret_cast<double(*)[P][N2][NACC]>(pool);
     __shared__ int s_nl[K_JCHUNK], s_n64[K_JCHUNK], s_c64[K_JCHUNK + 1], s_c32[K_JCHUNK + 1];
     const KChunk ch{s_nl, s_n64, s_c64, s_c32};
 
@@ -274,7 +310,7 @@ exchange_col_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KDensity d
             double s = 0.0;
             for (int w = 0; w < NW; w++)
                 for (int g = 0; g < P; g++) {
-                    if (ORI == 0) {
+                    if (S::O == 0) {
                         for (int d = 0; d < ND; d++) s += red[w][g][c * ND + d][a];
                     } else {
                         for (int b = 0; b < NB; b++) s += red[w][g][a * NB + b][c];
@@ -354,6 +390,7 @@ __device__ __forceinline__ int kcolc_group(bool act, int jg, int lg, const KPart
         QVT<T> q;
         T F[L + 1];
         make_quartet_t<L>(bg, kg, omega, tabs.f64, tabs.f32, q, F);
+        swap_lane_centre<ORI>(q);
         col_vrr_acc<LA, LB, LC, LD, ORI, T>(q, F, ln, acc, (T)w);
     }
     // HRRs and digestion once for the group pair; AB and CD from the first members
@@ -364,7 +401,7 @@ __device__ __forceinline__ int kcolc_group(bool act, int jg, int lg, const KPart
             CDz = (T)__ldg(cd.geo + G_RZ * cd.sp_stride + spl);
     if (lane_ok && ln.tidx >= 0) {
         T h[N2];
-        if (ORI == 0) hrr_bra_vector<LC, LD, T>(CDx, CDy, CDz, acc, h);
+        if (S::O == 0) hrr_bra_vector<LC, LD, T>(CDx, CDy, CDz, acc, h);
         else hrr_bra_vector<LA, LB, T>(ABx, ABy, ABz, acc, h);
 #pragma unroll
         for (int u = 0; u < N2; u++) U[ln.tidx][u] = (double)h[u];
@@ -380,11 +417,12 @@ __device__ __forceinline__ int kcolc_group(bool act, int jg, int lg, const KPart
                 T v[NXT];
 #pragma unroll
                 for (int x = 0; x < NXT; x++) v[x] = (T)U[x][u];
-                if (ORI == 0) {
+                if (S::O == 0) {
                     // unit = (c, d): bra HRR, then K[a][c] += sum_b (ab|cd) [Sij Skl] D[b][d]
                     const int dd = u % ND;
                     T I[NA * NB];
-                    hrr_bra_vector<LA, LB, T>(ABx, ABy, ABz, v, I);
+                    if constexpr (S::SW) hrr_bra_vector<LB, LA, T>(-ABx, -ABy, -ABz, v, I);
+                    else hrr_bra_vector<LA, LB, T>(ABx, ABy, ABz, v, I);
                     const double skl = ul ? 1.0 : (((mlm >> u) & 1ull) ? __ldg(cd.S + u * cd.sp_stride + spl) : 0.0);
                     const uint32_t lao = __ldg(dm.d_aoinds + lsh + (int64_t)dm.d_count * dd);
                     T wv[NB];
@@ -401,7 +439,7 @@ __device__ __forceinline__ int kcolc_group(bool act, int jg, int lg, const KPart
                             const T sij = uj ? (T)1 : (((mjm >> (a * NB + bq)) & 1ull)
                                                             ? (T)__ldg(ab.S + (a * NB + bq) * ab.sp_stride + spj)
                                                             : (T)0);
-                            sacc = fma(I[a * NB + bq] * sij, wv[bq], sacc);
+                            sacc = fma(I[S::iab(a, bq)] * sij, wv[bq], sacc);
                         }
                         Kacc[p][a] += (double)sacc;
                     }
@@ -409,7 +447,8 @@ __device__ __forceinline__ int kcolc_group(bool act, int jg, int lg, const KPart
                     // unit = (a, b): ket HRR, then K[a][c] += [Sij] sum_d (ab|cd) [Skl] D[b][d]
                     const int bb = u % NB;
                     T I[NC * ND];
-                    hrr_bra_vector<LC, LD, T>(CDx, CDy, CDz, v, I);
+                    if constexpr (S::SW) hrr_bra_vector<LD, LC, T>(-CDx, -CDy, -CDz, v, I);
+                    else hrr_bra_vector<LC, LD, T>(CDx, CDy, CDz, v, I);
                     const double sij = uj ? 1.0 : (((mjm >> u) & 1ull) ? __ldg(ab.S + u * ab.sp_stride + spj) : 0.0);
                     const uint32_t jao = __ldg(dm.b_aoinds + jsh + (int64_t)dm.b_count * bb);
                     T wv[ND];
@@ -426,7 +465,7 @@ __device__ __forceinline__ int kcolc_group(bool act, int jg, int lg, const KPart
                             const T skl = ul ? (T)1 : (((mlm >> (c * ND + d)) & 1ull)
                                                            ? (T)__ldg(cd.S + (c * ND + d) * cd.sp_stride + spl)
                                                            : (T)0);
-                            sacc = fma(I[c * ND + d] * skl, wv[d], sacc);
+                            sacc = fma(I[S::icd(c, d)] * skl, wv[d], sacc);
                         }
                         Kacc[p][c] += (double)sacc;
                     }
@@ -442,10 +481,12 @@ __device__ __forceinline__ int kcolc_group(bool act, int jg, int lg, const KPart
 // flattened partner enumeration, over partner groups instead of records (the
 // screen on group maxima selects a superset; kcolc_group applies the exact
 // per-member screen).  PM as for coulomb_kernel, split on the group maxima.
-// Registers are capped for 3 CTAs per SM (168): the heaviest classes spill a
-// little; a 2-CTA cap (no spills, fewer warps) measured no faster.
+// Registers are capped for 3 CTAs per SM (168) for the plain plans: the
+// heaviest classes spill a little; a 2-CTA cap (no spills, fewer warps)
+// measured no faster.  The packed plans (two or five quartets per warp, the
+// tower in registers) get the 2-CTA cap.
 template <int LA, int LB, int LC, int LD, int ORI, int PM>
-__global__ void __launch_bounds__(K_THREADS, 3)
+__global__ void __launch_bounds__(K_THREADS, ORI >= 2 ? 2 : 3)
 exchange_colc_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KGroups gab, KGroups gcd, KDensity dm,
                      double maxD, double omega, double thr, double* __restrict__ mat_K, BoysTabs tabs,
                      unsigned long long* __restrict__ qcount, double fp32_cut, double fp32_budget)
@@ -456,8 +497,9 @@ exchange_colc_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KGroups g
     constexpr int NW = K_THREADS / 32;
     constexpr int NL = S::NL, P = S::P, NXT = S::NXT;
     constexpr int N2 = S::N2, NACC = S::NACC, NPASS = S::NPASS;
-    __shared__ double U[NW][P][NXT][S::N2P];
-    __shared__ double red[NW][P][N2][NACC];
+    __shared__ double pool[S::POOL_DOUBLES];
+    double(*U)[P][NXT][S::N2P] = reinterpret_cast<double(*)[P][NXT][S::N2P]>(pool);
+    double(*red)[P][N2][NACC] = reinterpret_cast<double(*)[P][N2][NACC]>(pool);
     __shared__ int s_nl[K_JCHUNK], s_n64[K_JCHUNK], s_c64[K_JCHUNK + 1], s_c32[K_JCHUNK + 1];
     const KChunk ch{s_nl, s_n64, s_c64, s_c32};
 
@@ -524,7 +566,7 @@ exchange_colc_kernel(KOutBlocks out, KPartnerRecs ab, KPartnerRecs cd, KGroups g
             double sum = 0.0;
             for (int w = 0; w < NW; w++)
                 for (int g = 0; g < P; g++) {
-                    if (ORI == 0) {
+                    if (S::O == 0) {
                         for (int d = 0; d < ND; d++) sum += red[w][g][c * ND + d][a];
                     } else {
                         for (int b = 0; b < NB; b++) sum += red[w][g][a * NB + b][c];

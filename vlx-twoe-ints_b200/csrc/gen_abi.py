@@ -180,8 +180,14 @@ def header():
          "   copies, double-buffered; kind 1 = exchange: 0",
          "   one thread per quartet, 1 column kernel with bra lanes, 2 column kernel",
          "   with ket lanes, 3 / 4 the column kernels with bra / ket lanes that sum",
-         "   the primitive partners of one contracted shell before the HRR).  A",
-         "   column variant whose kernel does not fit the class falls back to 0.",
+         "   the primitive partners of one contracted shell before the HRR, 5 / 6",
+         "   packed column kernels with bra / ket lanes (lanes for the target",
+         "   levels only, from d up, so that a warp holds two or five quartets;",
+         "   the lower levels the VRR couples to are derived in each lane), 7 / 8",
+         "   the packed kernels with the lane-side pair built on its second",
+         "   centre (p+d and s+d pairs), 9..12 the contracted-partner kernels of",
+         "   the packed plans 5..8).  A column variant that is not built for",
+         "   the class, or whose kernel does not fit it, falls back to 0.",
          "   Every variant gives the same J/K to rounding; the",
          "   choice only changes speed.  Set by the autotuner.  No reference",
          "   counterpart. */",
@@ -194,7 +200,7 @@ def header():
          "   behaviour.  Process-wide.  No reference counterpart. */",
          "int vlxb_setFp32Cutoff(double cutoff);",
          "double vlxb_getFp32Cutoff(void);", "",
-         "/* FP32 error budget (with a cutoff > 0; default 2; 0 = no budget, the",
+         "/* FP32 error budget (with a cutoff > 0; default 0.5; 0 = no budget, the",
          "   cutoff alone decides).  A quartet below the cutoff runs in FP32 only inside the tail",
          "   of its list whose summed error proxy stays within `budget`: per J bra",
          "   record, |Q_ij| A_ij * sum over the FP32 kets of max|Q_kl D_kl| A_kl; per",

@@ -41,21 +41,45 @@ def level_comps(l0, l1):
     return out
 
 
+# Plan kinds ("ori"): bit 0 is the orientation (0: lanes = bra e, 1: lanes =
+# ket f); 2 and 3 are the packed plans of orientations 0 and 1 (lanes only
+# for the target levels, which must start at level 2: the level-1 coupling
+# partners come from the uniform tower, so a d+p lane side needs 16 lanes
+# instead of 20 and a warp holds two quartets); 4 and 5 are packed plans
+# whose lane-side pair is built on its second centre (B for the bra, D for
+# the ket: e in [lb, la + lb]), for the pairs whose second shell is the
+# higher one (p+d, s+d).  The kernels turn PA into PB = PA + AB and AB into
+# BA before the VRR (QC, CD likewise) and read the lane-side HRR result
+# transposed.
+PLAN_KINDS = range(6)
+
+
+def lane_pair(la, lb, lc, ld, ori):
+    """(first, second) shell of the lane-side pair and of the step-side pair."""
+    x, y = ((la, lb), (lc, ld)) if ori % 2 == 0 else ((lc, ld), (la, lb))
+    if ori >= 4:
+        x = (x[1], x[0])
+    return x, y
+
+
 class ColumnPlan:
     def __init__(self, la, lb, lc, ld, ori):
         self.cls = (la, lb, lc, ld)
         self.ori = ori
-        if ori == 0:
-            lx0, lx1, ly0, ly1 = la, la + lb, lc, lc + ld
-        else:
-            lx0, lx1, ly0, ly1 = lc, lc + ld, la, la + lb
+        self.orient = ori % 2
+        self.packed = ori >= 2
+        self.swapped = ori >= 4
+        (xa, xb), (ya, yb) = lane_pair(la, lb, lc, ld, ori)
+        lx0, lx1, ly0, ly1 = xa, xa + xb, ya, ya + yb
         self.lx0, self.lx1, self.ly0, self.ly1 = lx0, lx1, ly0, ly1
         self.L = la + lb + lc + ld
         self.lmin = max(0, lx0 - ly1)
-        lam = self.lmin
-        while len(level_comps(lam, lx1)) > 32:
-            lam += 1
-        assert lam - self.lmin <= 2, "derivation deeper than one level is not supported"
+        if self.packed:
+            lam = lx0
+        else:
+            lam = self.lmin
+            while len(level_comps(lam, lx1)) > 32:
+                lam += 1
         self.lam = lam
         self.lanes = level_comps(lam, lx1)          # lane side components, lane index = position
         self.NL = len(self.lanes)
@@ -63,9 +87,30 @@ class ColumnPlan:
         self.xtargets = level_comps(lx0, lx1)        # lane side targets
         self.ytargets = level_comps(ly0, ly1)        # step side targets
         self.derive = lam > self.lmin                 # level-lam lanes derive their coupling source
+        self.applies = self._applies()
+        if not self.applies:
+            return
+        assert lam - self.lmin <= 2, "derivation deeper than one level is not supported"
         self._step_closure()
         self._chain()
         self._tower()
+
+    def _applies(self):
+        """Whether this plan kind is built for the class: the plain kinds
+        always; a packed kind when its lanes start at level 2 below a
+        derivation (lam - 1 = 1, the tower's one-step partners), it holds more
+        quartets per warp than the plain plan of its orientation, and (for
+        4, 5) the lane-side pair's second shell is the higher one."""
+        if not self.packed:
+            return True
+        if self.lam != 2 or not self.derive or self.NL > 16:
+            return False
+        la, lb, lc, ld = self.cls
+        xa, xb = (la, lb) if self.orient == 0 else (lc, ld)
+        if self.swapped and not xa < xb:
+            return False
+        plain = ColumnPlan(la, lb, lc, ld, self.orient)
+        return self.P > plain.P
 
     # ---------------------------------------------------------- step nodes
     def _step_deps(self, y, m):
@@ -185,7 +230,7 @@ def emulate(plan: ColumnPlan, q: dict, F: list):
     """Run the column schedule for one quartet over plan.NL emulated lanes.
     q: quartet scalars (PAx.., WPx.., QCx.., WQx.., inv2z, inv2e, inv2ze, rz, re).
     Returns {(x, y): [x|y]^0} for x in lane targets, y in step targets."""
-    if plan.ori == 0:
+    if plan.orient == 0:
         PX, WX, i2X, rX = [q["PA" + c] for c in XYZ], [q["WP" + c] for c in XYZ], q["inv2z"], q["rz"]
         PY, WY, i2Y, rY = [q["QC" + c] for c in XYZ], [q["WQ" + c] for c in XYZ], q["inv2e"], q["re"]
     else:
@@ -258,14 +303,42 @@ def emulate(plan: ColumnPlan, q: dict, F: list):
 # CUDA emitter
 # ======================================================================
 
+K_JCHUNK = 256            # jk_kernels.cuh
+K_SMEM_LIMIT = 48 * 1024  # static shared memory of one kernel
+
+
 def k_smem_bytes(plan: ColumnPlan, warps: int = 4) -> int:
-    la, lb, lc, ld = plan.cls
+    """Static shared memory of the exchange column kernels: the lane-side HRR
+    rows U and the block's reduction buffer share one array (red is written
+    only after the block's last quartet), plus the chunk tables."""
+    if not plan.applies:
+        return 1 << 30
     na, nb, nc, nd = ((l + 1) * (l + 2) // 2 for l in plan.cls)
-    n2 = nc * nd if plan.ori == 0 else na * nb
-    nacc = na if plan.ori == 0 else nc
+    n2 = nc * nd if plan.orient == 0 else na * nb
+    nacc = na if plan.orient == 0 else nc
     U = warps * plan.P * len(plan.xtargets) * (n2 | 1) * 8
     red = warps * plan.P * n2 * nacc * 8
-    return U + red + (256 + 1) * 4
+    return max(U, red) + 4 * (K_JCHUNK + 1) * 4
+
+
+def k_fits(plan: ColumnPlan) -> bool:
+    return plan.applies and k_smem_bytes(plan) <= K_SMEM_LIMIT
+
+
+def k_variants(la, lb, lc, ld, spilling=False):
+    """Exchange kernel variants (schedule values) built for a class: 0 thread
+    per quartet (unless its code spills), 1 / 2 column with bra / ket lanes,
+    3 / 4 the contracted-partner column kernels, 5 / 6 packed column plans
+    (kinds 2 / 3), 7 / 8 packed plans on the second centre (kinds 4 / 5),
+    9..12 the contracted-partner kernels of kinds 2..5."""
+    out = [] if spilling else [0]
+    for ori in (0, 1):
+        if k_fits(ColumnPlan(la, lb, lc, ld, ori)):
+            out += [1 + ori, 3 + ori]
+    for ori in (2, 3, 4, 5):
+        if k_fits(ColumnPlan(la, lb, lc, ld, ori)):
+            out += [ori + 3, ori + 7]
+    return sorted(out)
 
 
 def _yname(y):
@@ -283,7 +356,14 @@ def emit_cuda(plan: ColumnPlan, T: str = "double", with_tables: bool = True, acc
     TT = T
     lit = "f" if T == "float" else ""
     T = f"{la}, {lb}, {lc}, {ld}, {ori}"
-    if ori == 0:
+    if not plan.applies:
+        if not with_tables:
+            return ""
+        return "\n".join([f"template <> struct ColTab<{T}> {{",
+                          "    static constexpr int NL = 1, P = 1, NXT = 1, NYT = 1, LAM = 0;",
+                          "    static constexpr bool K_FITS = false;  // plan kind not built for this class",
+                          "};", ""])
+    if plan.orient == 0:
         PX, WX, i2X, rX = ["q.PAx", "q.PAy", "q.PAz"], ["q.WPx", "q.WPy", "q.WPz"], "q.inv2z", "q.rz"
         PY, WY, i2Y, rY = ["q.QCx", "q.QCy", "q.QCz"], ["q.WQx", "q.WQy", "q.WQz"], "q.inv2e", "q.re"
     else:
@@ -299,7 +379,7 @@ def emit_cuda(plan: ColumnPlan, T: str = "double", with_tables: bool = True, acc
         L.append(f"template <> struct ColTab<{T}> {{")
         L.append(f"    static constexpr int NL = {plan.NL}, P = {plan.P}, NXT = {len(plan.xtargets)}, "
                  f"NYT = {len(plan.ytargets)}, LAM = {plan.lam};")
-        L.append(f"    static constexpr bool K_FITS = {'true' if k_smem_bytes(plan) <= 46 * 1024 else 'false'};"
+        L.append(f"    static constexpr bool K_FITS = {'true' if k_fits(plan) else 'false'};"
                  f"  // exchange kernel shared memory: {k_smem_bytes(plan)} bytes")
         L.append("};")
         L.append(f"__device__ const int8_t col_tab_{plan.name()}[{plan.NL}][20] = {{" + ", ".join(rows) + "};")
@@ -361,8 +441,14 @@ def emit_cuda(plan: ColumnPlan, T: str = "double", with_tables: bool = True, acc
         i = first_nz(y)
         y1 = sub1(y, i)
         nm = f"c{_yname(y)}_{m}"
-        L.append(f"    const {TT} sh_{nm} = __shfl_sync(0xffffffffu, {cname[(y1, m + 1)]}, ln.src[{i}]);")
-        cp = f"sh_{nm}"
+        # every lane at level lam (a packed plan over one level): the
+        # coupling source is always derived, no lane owns level lam - 1
+        one_level = plan.lx1 == plan.lam
+        if one_level:
+            cp = f"0.0{lit}"
+        else:
+            L.append(f"    const {TT} sh_{nm} = __shfl_sync(0xffffffffu, {cname[(y1, m + 1)]}, ln.src[{i}]);")
+            cp = f"sh_{nm}"
         if plan.need_derived[(y, m)]:
             g = y1
             gj = f"(jd{i} == 0 ? {g[0]}.0{lit} : (jd{i} == 1 ? {g[1]}.0{lit} : {g[2]}.0{lit}))"
@@ -371,7 +457,10 @@ def emit_cuda(plan: ColumnPlan, T: str = "double", with_tables: bool = True, acc
                 tl.append(tname[(sub1(g, j), m + 2)] if g[j] > 0 else f"0.0{lit}")
             tsel = f"(jd{i} == 0 ? {tl[0]} : (jd{i} == 1 ? {tl[1]} : {tl[2]}))"
             der = (f"fma({gj} * cpl, {tsel}, fma(jP{i}, {tname[(g, m + 1)]}, jW{i} * {tname[(g, m + 2)]}))")
-            L.append(f"    const {TT} cv_{nm} = ln.lamlane ? {der} : sh_{nm};")
+            if one_level:
+                L.append(f"    const {TT} cv_{nm} = {der};")
+            else:
+                L.append(f"    const {TT} cv_{nm} = ln.lamlane ? {der} : sh_{nm};")
             cp = f"cv_{nm}"
         e = f"fma({WY[i]}, {cname[(y1, m + 1)]}, {PY[i]} * {cname[(y1, m)]})"
         if y1[i] > 0:
@@ -413,7 +502,7 @@ def default_schedule():
         best = None
         for ori in (0, 1):
             p = ColumnPlan(*cls, ori)
-            if k_smem_bytes(p) > 46 * 1024:
+            if not k_fits(p):
                 continue
             util = p.P * p.NL / 32.0
             key = (-util, len(p.step_nodes) + len(p.tower_nodes))
@@ -438,14 +527,17 @@ def main(outdir):
     for cls in column_classes():
         name = "".join("spd"[l] for l in cls)
         parts = ["// Generated by gen_column.py -- do not edit.", "#pragma once", "namespace vlxb {", ""]
-        for ori in (0, 1):
-            parts.append(emit_cuda(ColumnPlan(*cls, ori), "double", True))
+        for ori in PLAN_KINDS:
+            plan = ColumnPlan(*cls, ori)
+            parts.append(emit_cuda(plan, "double", True))
             parts.append("")
-            parts.append(emit_cuda(ColumnPlan(*cls, ori), "float", False))
+            if not plan.applies:
+                continue
+            parts.append(emit_cuda(plan, "float", False))
             parts.append("")
-            parts.append(emit_cuda(ColumnPlan(*cls, ori), "double", False, acc=True))
+            parts.append(emit_cuda(plan, "double", False, acc=True))
             parts.append("")
-            parts.append(emit_cuda(ColumnPlan(*cls, ori), "float", False, acc=True))
+            parts.append(emit_cuda(plan, "float", False, acc=True))
             parts.append("")
         parts.append("}  // namespace vlxb")
         text = "\n".join(parts) + "\n"

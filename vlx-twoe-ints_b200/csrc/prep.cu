@@ -43,7 +43,7 @@ static std::mutex g_mu;
 static const double* g_boys_dev[64] = {nullptr};
 static const float* g_boys32_dev[64] = {nullptr};
 static std::atomic<double> g_fp32_cut{0.0};
-static std::atomic<double> g_fp32_budget{2.0};
+static std::atomic<double> g_fp32_budget{0.5};
 
 double fp32_cut_get() { return g_fp32_cut.load(std::memory_order_relaxed); }
 
@@ -167,7 +167,7 @@ int schedule_set(int kind, int la, int lb, int lc, int ld, int variant)
 {
     if (kind < 0 || kind > 1 || la < 0 || la > 2 || lb < 0 || lb > 2 || lc < 0 || lc > 2 || ld < 0 || ld > 2)
         return VLXB_EINVAL;
-    if (variant < 0 || variant > (kind == 0 ? 3 : 4)) return VLXB_EINVAL;
+    if (variant < 0 || variant > (kind == 0 ? 3 : 12)) return VLXB_EINVAL;
     std::call_once(g_sched_once, sched_init);
     g_sched[kind][la * 27 + lb * 9 + lc * 3 + ld].store(variant);
     return VLXB_OK;

@@ -2,7 +2,8 @@
 
 For each class and each compiled variant (J: thread-per-quartet, column,
 McMurchie-Davidson, thread-per-quartet with TMA-staged kets;
-K: thread-per-quartet, column with bra lanes, column with ket lanes) the class
+K: thread-per-quartet, column with bra or ket lanes, contracted column,
+packed column) the class
 entry point is timed with CUDA events on a given system's lists (best of
 `reps`), and the fastest variant is kept.  The result is a JSON schedule
 ({"J": {class: variant}, "K": {...}}) that `apply_schedule` loads into the
@@ -35,16 +36,12 @@ SPILLING_THREAD_KERNELS = {
 
 def compiled_variants(kind: str, cls: str):
     sys.path.insert(0, os.path.join(os.path.dirname(HERE), "csrc"))
-    from gen_column import ColumnPlan, k_smem_bytes
+    from gen_column import k_variants
 
     if kind == "J":
         return [1, 2] if cls in SPILLING_THREAD_KERNELS["J"] else [0, 1, 2, 3]
     l = [{"s": 0, "p": 1, "d": 2}[x] for x in cls]
-    out = [] if cls in SPILLING_THREAD_KERNELS["K"] else [0]
-    for ori in (0, 1):
-        if k_smem_bytes(ColumnPlan(*l, ori)) <= 46 * 1024:
-            out += [1 + ori, 3 + ori]
-    return out
+    return k_variants(*l, spilling=cls in SPILLING_THREAD_KERNELS["K"])
 
 
 def apply_schedule(path: str = DEFAULT_SCHEDULE) -> bool:
