@@ -104,6 +104,9 @@ def parse():
                     help="large leg: skip the FP64 reference build (errors against oracle/_ref rows only)")
     ap.add_argument("--batch-mols", type=int, default=32, help="batched leg: molecules (0 skips the leg)")
     ap.add_argument("--batch-atoms", type=int, nargs=2, default=(3, 8), help="batched leg: atom count range")
+    ap.add_argument("--fuse-group", type=int, default=64,
+                    help="batched leg: molecules per fused union (the fused regrouping's dense tables grow with "
+                         "the square of a union's primitive count)")
     ap.add_argument("--serve-reqs", type=int, default=12, help="served leg: requests per rate (0 skips the leg)")
     ap.add_argument("--serve-atoms", type=int, nargs=2, default=(5, 12), help="served leg: atom count range")
     ap.add_argument("--serve-iters", type=int, default=10, help="served leg: densities per request")
@@ -600,10 +603,15 @@ def run_batched(args, L, dev, cut):
     t_bmx = timed(bb.run, 3)
     L.set_fp32_cut(0.0)
     got = energies()
-    # fused: one class call per class for all molecules, one graph per iteration
-    from vlxb.batchfuse import FusedBatch
+    # fused: one class call per class for each union of up to --fuse-group
+    # molecules, one graph per iteration
+    from vlxb.batchfuse import FusedBatchGroups
 
-    fb = FusedBatch([w.mol for w in wls], [w.D for w in wls], 1e-12, device=dev)
+    # the per-molecule graph's memory is no longer needed
+    bb.graph = None
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    fb = FusedBatchGroups([w.mol for w in wls], [w.D for w in wls], 1e-12, device=dev, group=args.fuse_group)
     fb.capture()
     t_f64 = timed(fb.run, 3)
     fused_dE = 0.0
@@ -613,6 +621,8 @@ def run_batched(args, L, dev, cut):
         K = lists.contract_K(m.rl, fK)
         fused_dE = max(fused_dE, abs(lists.energy(wls[t].D, J, K) - ref[t][2]))
     L.set_fp32_cut(cut)
+    fb.graph = None
+    torch.cuda.empty_cache()
     fb.capture()
     t_fmx = timed(fb.run, 3)
     L.set_fp32_cut(0.0)
@@ -624,13 +634,14 @@ def run_batched(args, L, dev, cut):
             "speedup_batched_fp64": t_plain / t_b64, "speedup_batched_mixed": t_plain / t_bmx,
             "fused_fp64_builds_per_s": n / t_f64, "fused_mixed_builds_per_s": n / t_fmx,
             "speedup_fused_fp64": t_plain / t_f64, "speedup_fused_mixed": t_plain / t_fmx,
-            "fused_vs_batched_max_abs_dE_Eh": fused_dE,
+            "fused_vs_batched_max_abs_dE_Eh": fused_dE, "fused_unions": len(fb.parts),
             "max_abs_dJ": max(float(np.abs(a[0] - b[0]).max()) for a, b in zip(got, ref)),
             "max_abs_dK": max(float(np.abs(a[1] - b[1]).max()) for a, b in zip(got, ref)),
             "max_abs_dE_Eh": max(abs(a[2] - b[2]) for a, b in zip(got, ref)),
             "timing": ("device (CUDA events), best of 2-3 iterations; plain = sequential per-molecule builds; "
                        "batched = every molecule's class calls in one graph on 8 streams; fused = one class "
-                       "call per class for all molecules (vlxb_coulombBatch / vlxb_exchangeBatch), one graph")}
+                       "call per class per union of up to --fuse-group molecules (vlxb_coulombBatch / "
+                       "vlxb_exchangeBatch), one graph")}
 
 
 def run_served(args, L, dev, cut):

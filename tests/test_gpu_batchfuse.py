@@ -9,7 +9,7 @@ torch = pytest.importorskip("torch")
 
 from vlxb import basis, fock, lists
 from vlxb._lib import lib
-from vlxb.batchfuse import FusedBatch
+from vlxb.batchfuse import FusedBatch, FusedBatchGroups
 
 pytestmark = pytest.mark.gpu
 
@@ -66,3 +66,37 @@ def test_fused_batch_equals_per_molecule_calls():
     dJ0, dK0, _ = _direct(wls[0])
     _same(gJ0, dJ0)
     _same(gK0, dK0)
+
+
+def test_grouped_fused_batch_equals_per_molecule_calls():
+    """A batch split into fused unions of at most two molecules: every
+    molecule's J and K equal its own class calls, the quartet count equals
+    theirs, also from one captured graph over all groups and after a density
+    update."""
+    L = lib()
+    L.init(0)
+    wls = _mols(5, seed=3)
+    fg = FusedBatchGroups([w.mol for w in wls], [w.D for w in wls], 1e-12, group=2)
+    assert len(fg.parts) == 3 and fg.nmol == 5
+    fg.capture()
+    L.reset_counters()
+    fg.run()
+    torch.cuda.synchronize()
+    qf = sum(L.quartet_counters())
+    assert qf == fg.quartets_per_iteration
+    qd = 0
+    for t, wl in enumerate(wls):
+        dJ, dK, q = _direct(wl)
+        qd += q
+        gJ, gK = fg.results(t)
+        _same(gJ, dJ)
+        _same(gK, dK)
+    assert qf == qd
+    D3 = 0.8 * wls[3].D
+    fg.set_density(3, D3)
+    fg.run()
+    gJ, gK = fg.results(3)
+    p, k = fg.where[3]
+    dJ, dK, _ = _direct(wls[3], fg.parts[p].rls[k])
+    _same(gJ, dJ)
+    _same(gK, dK)

@@ -200,7 +200,7 @@ def header():
          "   behaviour.  Process-wide.  No reference counterpart. */",
          "int vlxb_setFp32Cutoff(double cutoff);",
          "double vlxb_getFp32Cutoff(void);", "",
-         "/* FP32 error budget (with a cutoff > 0; default 0.5; 0 = no budget, the",
+         "/* FP32 error budget (with a cutoff > 0; default 0.2; 0 = no budget, the",
          "   cutoff alone decides).  A quartet below the cutoff runs in FP32 only inside the tail",
          "   of its list whose summed error proxy stays within `budget`: per J bra",
          "   record, |Q_ij| A_ij * sum over the FP32 kets of max|Q_kl D_kl| A_kl; per",

@@ -43,7 +43,7 @@ static std::mutex g_mu;
 static const double* g_boys_dev[64] = {nullptr};
 static const float* g_boys32_dev[64] = {nullptr};
 static std::atomic<double> g_fp32_cut{0.0};
-static std::atomic<double> g_fp32_budget{0.5};
+static std::atomic<double> g_fp32_budget{0.2};
 
 double fp32_cut_get() { return g_fp32_cut.load(std::memory_order_relaxed); }
 

@@ -296,3 +296,66 @@ class FusedBatch:
         J = {k: self.matJ[k][slice(*self.jslices[k][m])].cpu().numpy() for k in rl.jlists}
         K = {k: self.matK[k][slice(*self.kslices[k][m])].cpu().numpy() for k in rl.kpairs}
         return J, K
+
+
+class FusedBatchGroups:
+    """A large batch as several fused unions of at most `group` molecules,
+    issued together (one graph for all of them with `capture`).
+
+    The device-side regrouping of a class call builds dense occupancy tables
+    over (first shell, second shell) of the call's primitives, whose size is
+    the product of the union's primitive counts: with 256 molecules of 3-8
+    atoms one union needs tables of about 1 GB per type pair and per class
+    call, and the whole iteration ran out of device memory.  Unions of 64
+    molecules keep each table 16 times smaller; the kernels, results and
+    quartet counts are those of FusedBatch on each group."""
+
+    def __init__(self, molecules, densities, threshold: float, device="cuda", group: int = 64, **kw):
+        if group < 1:
+            raise ValueError("group must be at least 1")
+        self.device = torch.device(device)
+        self.parts, self.where = [], []
+        for s in range(0, len(molecules), group):
+            fb = FusedBatch(molecules[s:s + group], densities[s:s + group], threshold, device=device, **kw)
+            self.where += [(len(self.parts), m) for m in range(fb.nmol)]
+            self.parts.append(fb)
+        self.nmol = len(self.where)
+        self.graph = None
+
+    def nbytes(self) -> int:
+        return sum(p.nbytes() for p in self.parts)
+
+    def issue(self, stream=None):
+        """Zero the outputs and queue one iteration of every group."""
+        for p in self.parts:
+            p.issue(stream)
+
+    def capture(self):
+        """Capture one iteration of all groups into one CUDA graph."""
+        s = torch.cuda.Stream(device=self.device)
+        L = self.parts[0].L
+        self.issue(s)
+        torch.cuda.synchronize(self.device)
+        L.reset_counters()
+        self.issue(s)
+        torch.cuda.synchronize(self.device)
+        qj, qk = L.quartet_counters(reset=True)
+        self.quartets_per_iteration = qj + qk
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            self.issue(s)
+        self.graph = g
+
+    def run(self):
+        if self.graph is None:
+            self.issue()
+        else:
+            self.graph.replay()
+
+    def set_density(self, m: int, D: np.ndarray):
+        p, k = self.where[m]
+        self.parts[p].set_density(k, D)
+
+    def results(self, m: int):
+        p, k = self.where[m]
+        return self.parts[p].results(k)
