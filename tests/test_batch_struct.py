@@ -67,3 +67,35 @@ def test_union_lists_slices_are_the_molecules_lists():
         a0 = u["ao0"][m]
         assert np.array_equal(h["Dstack"][a0:a0 + rl.naos, :rl.naos], rl.D_AO)
         assert np.all(h["mol0"][poff[0][m]:poff[0][m + 1]] == m)
+
+
+def test_fused_groups_split_and_map_molecules(monkeypatch):
+    """FusedBatchGroups splits a batch into unions of at most `group`
+    molecules in order and maps every molecule to its union and its index
+    there (the unions themselves replaced by a recording stand-in)."""
+    import pytest
+
+    from vlxb import batchfuse
+
+    made = []
+
+    class Stub:
+        def __init__(self, mols, dens, thr, device="cuda", **kw):
+            self.nmol = len(mols)
+            self.mols = list(mols)
+            made.append(self)
+
+        def results(self, m):
+            return self.mols[m]
+
+        def nbytes(self):
+            return 10 * self.nmol
+
+    monkeypatch.setattr(batchfuse, "FusedBatch", Stub)
+    mols = [f"m{t}" for t in range(7)]
+    fg = batchfuse.FusedBatchGroups(mols, [None] * 7, 1e-12, device="cpu", group=3)
+    assert [p.nmol for p in made] == [3, 3, 1] and fg.nmol == 7
+    assert [fg.results(t) for t in range(7)] == mols
+    assert fg.where[4] == (1, 1) and fg.nbytes() == 70
+    with pytest.raises(ValueError):
+        batchfuse.FusedBatchGroups(mols, [None] * 7, 1e-12, device="cpu", group=0)
