@@ -125,3 +125,52 @@ def test_generated_tables_match_variant_list(tmp_path):
             assert fits[ori] == ({1 + ori, 3 + ori} <= kv), (cls, ori)
         for ori in (2, 3, 4, 5):
             assert fits[ori] == ({ori + 3, ori + 7} <= kv), (cls, ori)
+
+
+def _hrr(col, R, l1, l2):
+    """(x y| for x of level l1, y of level l2 from e = x + y values on the
+    first centre: (x, y + 1_i) = (x + 1_i, y) + R_i (x, y), R = first - second."""
+
+    @functools.lru_cache(maxsize=None)
+    def h(x, y):
+        if sum(y) == 0:
+            return col[x]
+        i = next(k for k in range(3) if y[k] > 0)
+        y1 = tuple(y[k] - (k == i) for k in range(3))
+        x1 = tuple(x[k] + (k == i) for k in range(3))
+        return h(x1, y1) + R[i] * h(x, y1)
+
+    return {(x, y): h(tuple(x), tuple(y)) for x in gc.level_comps(l1, l1) for y in gc.level_comps(l2, l2)}
+
+
+@pytest.mark.parametrize("cls,ori", [("pddd", 4), ("pdpd", 4), ("pdpd", 5), ("sddd", 4)])
+def test_second_centre_plan_gives_the_same_integrals(cls, ori):
+    """A second-centre plan (the lane-side pair built on B, or D) with PA
+    turned into PB = PA + AB and the HRR run from B to A with R = BA, read
+    transposed, gives the plain plan's (a b| (or |c d)) for every step-side
+    target: the transformation the column kernels apply before and after the
+    packed VRR."""
+    l = tuple({"s": 0, "p": 1, "d": 2}[x] for x in cls)
+    orient = ori % 2
+    plain, swapped = gc.ColumnPlan(*l, orient), gc.ColumnPlan(*l, ori)
+    assert swapped.applies
+    rng = np.random.default_rng(zlib.crc32(f"swap{cls}{ori}".encode()))
+    keys = [p + c for p in ("PA", "WP", "QC", "WQ") for c in XYZ]
+    q = {k: float(rng.uniform(-1.0, 1.0)) for k in keys}
+    q.update(inv2z=float(rng.uniform(0.2, 1.0)), inv2e=float(rng.uniform(0.2, 1.0)),
+             inv2ze=float(rng.uniform(0.1, 0.5)), rz=float(rng.uniform(0.2, 0.8)), re=float(rng.uniform(0.2, 0.8)))
+    R = [float(v) for v in rng.uniform(-1.0, 1.0, 3)]  # AB (orientation 0) or CD (orientation 1)
+    F = [float(rng.uniform(0.1, 1.0)) / (m + 1) for m in range(plain.L + 1)]
+    P = "PA" if orient == 0 else "QC"
+    q2 = dict(q)
+    for t, c in enumerate(XYZ):
+        q2[P + c] = q[P + c] + R[t]
+    a = gc.emulate(plain, q, F)
+    b = gc.emulate(swapped, q2, F)
+    l1, l2 = (l[0], l[1]) if orient == 0 else (l[2], l[3])
+    for y in plain.ytargets:
+        ab = _hrr({x: a[(x, y)] for x in plain.xtargets}, R, l1, l2)
+        ba = _hrr({x: b[(x, y)] for x in swapped.xtargets}, [-r for r in R], l2, l1)
+        for (x1, x2), v in ab.items():
+            w = ba[(x2, x1)]
+            assert abs(v - w) <= 1e-11 * max(1.0, abs(v)), (cls, ori, x1, x2, y, v, w)
